@@ -1,0 +1,737 @@
+// gila.cu -- C ABI of libgila_b200: contexts, operators, the matvec entry
+// points.  Construction mirrors GlaOprMem / GlaOprPrp (src/glaMemSup.jl:16-269),
+// the apply mirrors egoOpr! (src/glaAct.jl:33-49) and mul! (src/glaLinAlg.jl).
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <complex>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+namespace gila {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+gila_status fail(gila_status s, const std::string& msg) {
+  g_err = msg;
+  return s;
+}
+gila_status cuda_fail(cudaError_t e, const char* where) {
+  g_err = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") at " + where;
+  if (e == cudaErrorMemoryAllocation) return GILA_ERR_NOMEM;
+  return GILA_ERR_CUDA;
+}
+
+size_t csize(gila_dtype t) { return t == GILA_C128 ? 16 : 8; }
+
+// ------------------------------------------------------------- rationals
+static int64_t gcd64(int64_t a, int64_t b) {
+  a = a < 0 ? -a : a;
+  b = b < 0 ? -b : b;
+  while (b) {
+    int64_t t = a % b;
+    a = b;
+    b = t;
+  }
+  return a;
+}
+Rat rat(int64_t n, int64_t d) {
+  if (d < 0) {
+    n = -n;
+    d = -d;
+  }
+  int64_t g = gcd64(n, d);
+  if (g == 0) g = 1;
+  return Rat{n / g, d / g};
+}
+bool rat_eq(Rat a, Rat b) { return a.n == b.n && a.d == b.d; }
+static Rat rdiv(Rat a, Rat b) { return rat(a.n * b.d, a.d * b.n); }
+static bool risint(Rat a) { return a.d == 1; }
+
+Vol vol_from_abi(const gila_vol& v) {
+  Vol o;
+  for (int k = 0; k < 3; ++k) {
+    o.cel[k] = v.cel[k];
+    o.scl[k] = rat(v.scl_num[k], v.scl_den[k]);
+    o.org[k] = rat(v.org_num[k], v.org_den[k]);
+    if (v.grd_den[k] == 0)
+      o.grd[k] = o.scl[k];
+    else
+      o.grd[k] = rat(v.grd_num[k], v.grd_den[k]);
+  }
+  return o;
+}
+gila_vol vol_to_abi(const Vol& v) {
+  gila_vol o;
+  for (int k = 0; k < 3; ++k) {
+    o.cel[k] = v.cel[k];
+    o.scl_num[k] = v.scl[k].n;
+    o.scl_den[k] = v.scl[k].d;
+    o.org_num[k] = v.org[k].n;
+    o.org_den[k] = v.org[k].d;
+    o.grd_num[k] = v.grd[k].n;
+    o.grd_den[k] = v.grd[k].d;
+  }
+  return o;
+}
+bool vol_eq(const Vol& a, const Vol& b) {
+  for (int k = 0; k < 3; ++k)
+    if (a.cel[k] != b.cel[k] || !rat_eq(a.scl[k], b.scl[k]) || !rat_eq(a.org[k], b.org[k]) ||
+        !rat_eq(a.grd[k], b.grd[k]))
+      return false;
+  return true;
+}
+
+// glaVolEveGen (src/glaMem.jl:152-175)
+Vol vol_even(const Vol& v) {
+  bool all_even = true;
+  for (int k = 0; k < 3; ++k) all_even &= (v.cel[k] % 2 == 0);
+  if (all_even) return v;
+  Vol o = v;
+  for (int k = 0; k < 3; ++k) {
+    const int64_t par = v.cel[k] % 2;
+    const int64_t nc = v.cel[k] + par;
+    o.cel[k] = nc;
+    o.scl[k] = rat(v.scl[k].n * v.cel[k], v.scl[k].d * nc);
+    o.grd[k] = rat(v.grd[k].n * v.cel[k], v.grd[k].d * nc);
+  }
+  return o;
+}
+
+// GlaExtInf constructor (src/glaMem.jl:190-216)
+gila_status ext_inf(const Vol& trg, const Vol& src, ExtInf* out) {
+  int64_t ok = 1;
+  for (int k = 0; k < 3; ++k) ok *= (int)risint(rdiv(src.scl[k], trg.scl[k])) + (int)risint(rdiv(trg.scl[k], src.scl[k]));
+  if (ok == 0) return fail(GILA_ERR_SCALE, "Volume pair must share a common scale grid.");
+  for (int k = 0; k < 3; ++k) {
+    const Rat a = src.scl[k], b = trg.scl[k];
+    const int64_t gn = gcd64(a.n, b.n), ld = a.d / gcd64(a.d, b.d) * b.d;
+    out->min_scl[k] = rat(gn, ld);
+    const int64_t ln = a.n / gcd64(a.n, b.n) * b.n, gd = gcd64(a.d, b.d);
+    const Rat mx = rat(ln, gd);
+    const Rat td = rdiv(mx, trg.scl[k]), sd = rdiv(mx, src.scl[k]);
+    out->tdiv[k] = (int)(td.n / td.d);
+    out->sdiv[k] = (int)(sd.n / sd.d);
+    out->tc[k] = (int)(trg.cel[k] / out->tdiv[k]);
+    out->sc[k] = (int)(src.cel[k] / out->sdiv[k]);
+    if (out->tc[k] == 0 || out->sc[k] == 0)
+      return fail(GILA_ERR_SCALE, "Volume sizes are incompatible---volume smaller than cell.");
+  }
+  return GILA_OK;
+}
+
+// ------------------------------------------------------------ FFT plans
+gila_status plan_axis(int P, AxisPlan* pl) {
+  pl->P = P;
+  pl->nst = 0;
+  int r = P;
+  int twos = 0;
+  while (r % 2 == 0) {
+    r /= 2;
+    ++twos;
+  }
+  while (twos >= 3) {
+    pl->radix[pl->nst++] = 8;
+    twos -= 3;
+  }
+  if (twos == 2) pl->radix[pl->nst++] = 4;
+  if (twos == 1) pl->radix[pl->nst++] = 2;
+  for (int q : {3, 5, 7}) {
+    while (r % q == 0) {
+      if (pl->nst >= 12) return fail(GILA_ERR_ARG, "axis length has too many factors");
+      pl->radix[pl->nst++] = q;
+      r /= q;
+    }
+  }
+  if (r != 1)
+    return fail(GILA_ERR_ARG, "circulant length " + std::to_string(P) +
+                                  " has a prime factor above 7; supported lengths are 2^a 3^b 5^c 7^d");
+  if (pl->nst == 0) pl->radix[pl->nst++] = 2;  // P == 1 cannot occur (P even)
+  return GILA_OK;
+}
+
+gila_status twiddle_table(Ctx* ctx, int P, gila_dtype dt, const void** out) {
+  std::lock_guard<std::mutex> lk(ctx->mu);
+  auto key = std::make_pair(P, (int)dt);
+  auto it = ctx->tw_cache.find(key);
+  if (it != ctx->tw_cache.end()) {
+    *out = it->second;
+    return GILA_OK;
+  }
+  // w_P^m = exp(-2 pi i m / P); angle reduced to the first octant for accuracy
+  std::vector<double> re(P), im(P);
+  for (int m = 0; m < P; ++m) {
+    const long double a = -2.0L * 3.14159265358979323846264338327950288L * (long double)m / (long double)P;
+    re[m] = (double)cosl(a);
+    im[m] = (double)sinl(a);
+  }
+  void* d = nullptr;
+  const size_t bytes = (size_t)P * csize(dt);
+  GILA_CUDA_TRY(cudaMalloc(&d, bytes));
+  if (dt == GILA_C128) {
+    std::vector<double2> h(P);
+    for (int m = 0; m < P; ++m) h[m] = make_double2(re[m], im[m]);
+    GILA_CUDA_TRY(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float2> h(P);
+    for (int m = 0; m < P; ++m) h[m] = make_float2((float)re[m], (float)im[m]);
+    GILA_CUDA_TRY(cudaMemcpy(d, h.data(), bytes, cudaMemcpyHostToDevice));
+  }
+  ctx->tw_cache[key] = d;
+  *out = d;
+  return GILA_OK;
+}
+
+Ctx::~Ctx() {
+  for (auto& kv : tw_cache) cudaFree(kv.second);
+}
+
+Core::~Core() {
+  if (device >= 0) cudaSetDevice(device);
+  if (stream) cudaStreamSynchronize(stream);
+  cudaFree(ker);
+  for (int k = 0; k < 3; ++k) cudaFree(maps[k]);
+  cudaFree(A);
+  cudaFree(B);
+  cudaFree(stage_in);
+  cudaFree(stage_out);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// Stored kernel extents (src/glaMemSup.jl:121-136).
+static void tru_inf(const Core& c, int tru[3]) {
+  for (int d = 0; d < 3; ++d) {
+    const int tot = c.mix.tc[d] + c.mix.sc[d];
+    const bool one_par = (c.mix.sdiv[0] * c.mix.sdiv[1] * c.mix.sdiv[2] == 1) &&
+                         (c.mix.tdiv[0] * c.mix.tdiv[1] * c.mix.tdiv[2] == 1);
+    if (c.mix.tc[d] == c.mix.sc[d] && one_par && rat_eq(c.trg.org[d], c.src.org[d])) {
+      const int n = c.mix.tc[d];
+      const int v = (n + 1) / 2 + (n % 2 == 0 ? 1 : 0);
+      tru[d] = v > 2 ? v : 2;
+    } else {
+      tru[d] = tot / 2;
+    }
+  }
+}
+
+// Per-frequency kernel address on one axis, following the forward / reverse
+// quadrants of mulBrnDev! (src/glaActSup.jl:789-846): frequency f = 2k + p
+// reads stored index m of branch p, mirrored (sign flip for off-diagonal
+// components) in the reverse quadrant.
+static std::vector<int> axis_map(int P, int tru, int tcel) {
+  const int brn = P / 2;
+  std::vector<int> m(P);
+  for (int f = 0; f < P; ++f) {
+    const int p = f % 2, k = f / 2;
+    int idx = k, mir = 0;
+    if (tru != brn) {
+      const int fwd_even = (tcel + 1) / 2 + (tcel % 2 == 0 ? 1 : 0);
+      const int fwd_odd = (tcel + 1) / 2;
+      if (p == 0 && k >= fwd_even) {
+        idx = brn - k;
+        mir = 1;
+      } else if (p == 1 && k >= fwd_odd) {
+        idx = brn - 1 - k;
+        mir = 1;
+      }
+    }
+    m[f] = idx | (p << 29) | (mir << 30);
+  }
+  return m;
+}
+
+static gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* src_abi, const gila_kopt* opt,
+                             gila_dtype dtype, std::shared_ptr<Core>& core) {
+  if (!ctx || !trg_abi) return fail(GILA_ERR_ARG, "null context or target volume");
+  if (dtype != GILA_C64 && dtype != GILA_C128) return fail(GILA_ERR_TYPE, "setTyp must be ComplexF32 or ComplexF64");
+  core = std::make_shared<Core>();
+  core->ctx = ctx->impl;
+  core->device = ctx->impl->device;
+  core->dtype = dtype;
+  if (opt)
+    core->opt = *opt;
+  else {
+    core->opt.frq_re = 1.0;
+    core->opt.frq_im = 0.0;
+    core->opt.int_ord = 32;
+    core->opt.dev_mod = 1;
+  }
+  Vol trg = vol_from_abi(*trg_abi);
+  for (int k = 0; k < 3; ++k)
+    if (trg.cel[k] <= 0) return fail(GILA_ERR_ARG, "cell counts must be positive");
+  Vol src = src_abi ? vol_from_abi(*src_abi) : trg;
+  // self / external detection and even-cell regeneration (src/glaMemSup.jl:26-43)
+  if (!src_abi || vol_eq(trg, src)) {
+    core->self = true;
+    src = trg;
+  } else {
+    core->self = false;
+    int64_t odd = 0;
+    for (int k = 0; k < 3; ++k) odd += (trg.cel[k] + src.cel[k]) % 2;
+    if (odd != 0) {
+      fprintf(stderr,
+              "Warning! A volume has been regenerated to have an even number of cells---the size of a cell has "
+              "changed. The sum of the number of source and target cells must be even for the algorithm to "
+              "function.\n");
+      trg = vol_even(trg);
+      src = vol_even(src);
+    }
+  }
+  core->trg = trg;
+  core->src = src;
+  gila_status s = ext_inf(trg, src, &core->mix);
+  if (s != GILA_OK) return s;
+  core->parS = core->mix.sdiv[0] * core->mix.sdiv[1] * core->mix.sdiv[2];
+  Geom& g = core->geom;
+  int parT = core->mix.tdiv[0] * core->mix.tdiv[1] * core->mix.tdiv[2];
+  if (parT > 64) return fail(GILA_ERR_ARG, "more than 64 target partitions are not supported");
+  g.parT = parT;
+  for (int k = 0; k < 3; ++k) {
+    g.sc[k] = core->mix.sc[k];
+    g.tc[k] = core->mix.tc[k];
+    g.P[k] = g.sc[k] + g.tc[k];
+    g.tdiv[k] = core->mix.tdiv[k];
+    g.out_full[k] = (int64_t)g.tc[k] * g.tdiv[k];
+  }
+  int t = 0;
+  for (int z = 0; z < g.tdiv[2]; ++z)
+    for (int y = 0; y < g.tdiv[1]; ++y)
+      for (int x = 0; x < g.tdiv[0]; ++x, ++t) {
+        g.toff[t][0] = x;
+        g.toff[t][1] = y;
+        g.toff[t][2] = z;
+      }
+  tru_inf(*core, g.tru);
+  for (int k = 0; k < 3; ++k) {
+    if ((s = plan_axis(g.P[k], &core->plan[k])) != GILA_OK) return s;
+    if ((s = twiddle_table(ctx->impl, g.P[k], dtype, &core->tw[k])) != GILA_OK) return s;
+    std::vector<int> m = axis_map(g.P[k], g.tru[k], g.tc[k]);
+    GILA_CUDA_TRY(cudaMalloc(&core->maps[k], m.size() * sizeof(int)));
+    GILA_CUDA_TRY(cudaMemcpy(core->maps[k], m.data(), m.size() * sizeof(int), cudaMemcpyHostToDevice));
+  }
+  GILA_CUDA_TRY(cudaStreamCreateWithFlags(&core->stream, cudaStreamNonBlocking));
+  return GILA_OK;
+}
+
+static bool is_device_ptr(const void* p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+// Re-layout the reference egoFur (tx,ty,tz,6,parS,parT column-major, one
+// array per branch eo) into [parT][eo][tz][ty][tx][6] of the operator dtype.
+template <typename CT>
+static gila_status load_fur(Core& c, const void* const fur[8], gila_dtype fdt, std::vector<CT>& out) {
+  const Geom& g = c.geom;
+  const int tx = g.tru[0], ty = g.tru[1], tz = g.tru[2];
+  const int64_t per = (int64_t)tx * ty * tz * 6;
+  out.assign((size_t)per * 8 * g.parT, CT{});
+  const int64_t n_in = per * c.parS * g.parT;
+  std::vector<unsigned char> host;
+  for (int eo = 0; eo < 8; ++eo) {
+    const void* src = fur[eo];
+    if (!src) return fail(GILA_ERR_ARG, "null egoFur branch");
+    const size_t bytes = (size_t)n_in * csize(fdt);
+    const unsigned char* hp;
+    if (is_device_ptr(src)) {
+      host.resize(bytes);
+      GILA_CUDA_TRY(cudaMemcpy(host.data(), src, bytes, cudaMemcpyDeviceToHost));
+      hp = host.data();
+    } else {
+      hp = static_cast<const unsigned char*>(src);
+    }
+    for (int tp = 0; tp < g.parT; ++tp)
+      for (int cc = 0; cc < 6; ++cc)
+        for (int iz = 0; iz < tz; ++iz)
+          for (int iy = 0; iy < ty; ++iy)
+            for (int ix = 0; ix < tx; ++ix) {
+              // source partition 0 only (parS > 1 operators cannot be applied)
+              const int64_t si = ((((int64_t)tp * c.parS + 0) * 6 + cc) * tz + iz) * ty * (int64_t)tx +
+                                 (int64_t)iy * tx + ix;
+              double re, im;
+              if (fdt == GILA_C128) {
+                const double* q = reinterpret_cast<const double*>(hp) + 2 * si;
+                re = q[0];
+                im = q[1];
+              } else {
+                const float* q = reinterpret_cast<const float*>(hp) + 2 * si;
+                re = q[0];
+                im = q[1];
+              }
+              if (!std::isfinite(re) || !std::isfinite(im))
+                return fail(GILA_ERR_NAN, "Fourier information contains non-numeric values.");
+              const int64_t di = (((((int64_t)tp * 8 + eo) * tz + iz) * ty + iy) * tx + ix) * 6 + cc;
+              out[di].x = (decltype(out[di].x))re;
+              out[di].y = (decltype(out[di].y))im;
+            }
+  }
+  return GILA_OK;
+}
+
+template <typename C>
+static DevOp<C> devop(const Core& c) {
+  DevOp<C> d;
+  d.ker = static_cast<const C*>(c.ker);
+  for (int k = 0; k < 3; ++k) {
+    d.map[k] = c.maps[k];
+    d.tw[k] = static_cast<const C*>(c.tw[k]);
+    d.plan[k] = c.plan[k];
+  }
+  d.scale = 1.0 / ((double)c.geom.P[0] * c.geom.P[1] * c.geom.P[2]);
+  return d;
+}
+
+// Launch shapes: the largest tiles whose thread count stays <= 512 with 8
+// staged values per thread and whose shared memory stays within budget.
+static Launch default_launch(const Core& c) {
+  const Geom& g = c.geom;
+  const int cs = (int)csize(c.dtype);
+  Launch L;
+  auto lines = [&](int P) {
+    int m = 2048 / P;
+    if (m < 1) m = 1;
+    while (m > 1 && ((m * P + 7) / 8 > 512)) --m;
+    return m;
+  };
+  L.xf_lines = lines(g.P[0]);
+  L.xi_lines = lines(g.P[0]);
+  auto tile = [&](int P, int ch, int want, int smem_budget) {
+    int tx = want;
+    while (tx > 1 && (((ch * tx * P + 7) / 8) > 512 || (int64_t)ch * tx * P * cs > smem_budget)) tx /= 2;
+    if (tx > g.P[0]) tx = g.P[0];
+    return tx < 1 ? 1 : tx;
+  };
+  const int want = c.dtype == GILA_C128 ? 8 : 16;
+  L.y_tx = tile(g.P[1], 1, want, 96 * 1024);
+  L.z_tx = tile(g.P[2], 3 * (g.parT > 1 ? 2 : 1), want, 110 * 1024);
+  return L;
+}
+
+static gila_status ensure_work(Core& c, int64_t nrhs) {
+  if (nrhs <= c.cap_rhs) return GILA_OK;
+  const Work w = work_sizes(c.geom);
+  const size_t cs = csize(c.dtype);
+  cudaFree(c.A);
+  cudaFree(c.B);
+  c.A = c.B = nullptr;
+  c.cap_rhs = 0;
+  GILA_CUDA_TRY(cudaMalloc(&c.A, (size_t)(w.a_rhs * nrhs) * cs));
+  GILA_CUDA_TRY(cudaMalloc(&c.B, (size_t)(w.b_rhs * nrhs) * cs));
+  c.cap_rhs = nrhs;
+  return GILA_OK;
+}
+
+static int64_t in_elems(const Core& c) { return 3LL * c.geom.sc[0] * c.geom.sc[1] * c.geom.sc[2]; }
+static int64_t out_elems(const Core& c) {
+  return 3LL * c.geom.out_full[0] * c.geom.out_full[1] * c.geom.out_full[2];
+}
+
+template <typename C>
+static gila_status apply_t(Core& c, const void* in, void* out, int64_t nrhs, bool axpby, const double* alpha,
+                           const double* beta, cudaStream_t user_st) {
+  const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
+  const size_t cs = sizeof(C);
+  gila_status s = ensure_work(c, nrhs);
+  if (s != GILA_OK) return s;
+  if (!c.tuned) {
+    c.launch = default_launch(c);
+    c.tuned = true;
+  }
+  cudaStream_t st = user_st ? user_st : c.stream;
+  const bool din = is_device_ptr(in), dout = is_device_ptr(out);
+  const C* d_in = static_cast<const C*>(in);
+  C* d_out = static_cast<C*>(out);
+  if (!din) {
+    if (c.stage_cap_in < ni) {
+      cudaFree(c.stage_in);
+      c.stage_in = nullptr;
+      c.stage_cap_in = 0;
+      GILA_CUDA_TRY(cudaMalloc(&c.stage_in, (size_t)ni * cs));
+      c.stage_cap_in = ni;
+    }
+    GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_in, in, (size_t)ni * cs, cudaMemcpyHostToDevice, st));
+    d_in = static_cast<const C*>(c.stage_in);
+  }
+  if (!dout) {
+    if (c.stage_cap_out < no) {
+      cudaFree(c.stage_out);
+      c.stage_out = nullptr;
+      c.stage_cap_out = 0;
+      GILA_CUDA_TRY(cudaMalloc(&c.stage_out, (size_t)no * cs));
+      c.stage_cap_out = no;
+    }
+    if (axpby) GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_out, out, (size_t)no * cs, cudaMemcpyHostToDevice, st));
+    d_out = static_cast<C*>(c.stage_out);
+  }
+  C a, b;
+  a.x = alpha ? (decltype(a.x))alpha[0] : 1;
+  a.y = alpha ? (decltype(a.y))alpha[1] : 0;
+  b.x = beta ? (decltype(b.x))beta[0] : 0;
+  b.y = beta ? (decltype(b.y))beta[1] : 0;
+  GILA_CUDA_TRY(launch_matvec<C>(c.geom, devop<C>(c), c.launch, d_in, d_out, static_cast<C*>(c.A),
+                                 static_cast<C*>(c.B), (int)nrhs, axpby, a, b, st));
+  if (!dout) GILA_CUDA_TRY(cudaMemcpyAsync(out, c.stage_out, (size_t)no * cs, cudaMemcpyDeviceToHost, st));
+  if (!user_st || !din || !dout) GILA_CUDA_TRY(cudaStreamSynchronize(st));
+  return GILA_OK;
+}
+
+static gila_status apply_common(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len, void* out,
+                                int64_t out_len, int64_t nrhs, bool axpby, const double* alpha, const double* beta,
+                                void* stream) {
+  if (!opr || !opr->core) return fail(GILA_ERR_ARG, "null operator");
+  Core& c = *opr->core;
+  if (dtype != c.dtype)
+    return fail(GILA_ERR_TYPE, std::string("Input array must have the same element type as the operator. eltype(opr) = ") +
+                                   (c.dtype == GILA_C128 ? "ComplexF64" : "ComplexF32"));
+  if (nrhs < 1) return fail(GILA_ERR_ARG, "nrhs must be >= 1");
+  if (c.parS != 1 || in_len != in_elems(c) * nrhs || out_len != out_elems(c) * nrhs)
+    return fail(GILA_ERR_SIZE,
+                "Size of input vector does not match size of source volume. Required data layout is (srcCelX, "
+                "srcCelY, srcCelZ, 3).");
+  if (!in || !out) return fail(GILA_ERR_ARG, "null vector");
+  std::lock_guard<std::mutex> lk(c.mu);
+  GILA_CUDA_TRY(cudaSetDevice(c.device));
+  if (c.dtype == GILA_C128)
+    return apply_t<double2>(c, in, out, nrhs, axpby, alpha, beta, static_cast<cudaStream_t>(stream));
+  return apply_t<float2>(c, in, out, nrhs, axpby, alpha, beta, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace gila
+
+using namespace gila;
+
+// =================================================================== C ABI
+extern "C" {
+
+const char* gila_last_error(void) { return g_err.c_str(); }
+
+const char* gila_version(void) { return "0.1.0"; }
+
+const char* gila_status_string(gila_status s) {
+  switch (s) {
+    case GILA_OK: return "ok";
+    case GILA_ERR_ARG: return "invalid argument";
+    case GILA_ERR_SIZE: return "size mismatch";
+    case GILA_ERR_TYPE: return "element type mismatch";
+    case GILA_ERR_CUDA: return "CUDA error";
+    case GILA_ERR_NOMEM: return "out of memory";
+    case GILA_ERR_NAN: return "non-numeric values";
+    case GILA_ERR_NODEV: return "no usable CUDA device";
+    case GILA_ERR_OVERLAP: return "overlapping volumes";
+    case GILA_ERR_SCALE: return "incompatible scales";
+    case GILA_ERR_NOTCONV: return "not converged";
+    case GILA_ERR_TIMEOUT: return "device wait timed out";
+    default: return "internal error";
+  }
+}
+
+gila_status gila_ctx_create(int device, gila_ctx** out) {
+  if (!out) return fail(GILA_ERR_ARG, "null output");
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    cudaGetLastError();
+    return fail(GILA_ERR_NODEV,
+                "Device computation requested, but CUDA is not functional. For CPU computation use "
+                "GlaKerOpt(false)---devMod = false---when declaring compute options.");
+  }
+  if (device < 0 || device >= n) return fail(GILA_ERR_ARG, "device index out of range");
+  GILA_CUDA_TRY(cudaSetDevice(device));
+  GILA_CUDA_TRY(cudaFree(0));
+  auto* c = new gila_ctx;
+  c->impl = new Ctx;
+  c->impl->device = device;
+  *out = c;
+  return GILA_OK;
+}
+
+gila_status gila_ctx_destroy(gila_ctx* ctx) {
+  if (!ctx) return GILA_OK;
+  cudaSetDevice(ctx->impl->device);
+  delete ctx->impl;
+  delete ctx;
+  return GILA_OK;
+}
+
+gila_status gila_opr_create_from_fur(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src, const gila_kopt* opt,
+                                     gila_dtype dtype, const void* const fur[8], const int64_t fur_dims[8][6],
+                                     gila_dtype fur_dtype, gila_opr** out) {
+  if (!out || !fur || !fur_dims) return fail(GILA_ERR_ARG, "null argument");
+  if (!ctx) return fail(GILA_ERR_ARG, "null context");
+  GILA_CUDA_TRY(cudaSetDevice(ctx->impl->device));
+  std::shared_ptr<Core> core;
+  gila_status s = init_core(ctx, trg, src, opt, dtype, core);
+  if (s != GILA_OK) return s;
+  const Geom& g = core->geom;
+  for (int eo = 0; eo < 8; ++eo) {
+    const int64_t want[6] = {g.tru[0], g.tru[1], g.tru[2], 6, core->parS, g.parT};
+    for (int k = 0; k < 6; ++k)
+      if (fur_dims[eo][k] != want[k])
+        return fail(GILA_ERR_ARG, "egoFur branch " + std::to_string(eo) + " has extents that do not match the volumes");
+  }
+  const size_t bytes = (size_t)g.tru[0] * g.tru[1] * g.tru[2] * 6 * 8 * g.parT * csize(dtype);
+  GILA_CUDA_TRY(cudaMalloc(&core->ker, bytes));
+  core->ker_bytes = bytes;
+  if (dtype == GILA_C128) {
+    std::vector<double2> h;
+    if ((s = load_fur(*core, fur, fur_dtype, h)) != GILA_OK) return s;
+    GILA_CUDA_TRY(cudaMemcpy(core->ker, h.data(), bytes, cudaMemcpyHostToDevice));
+  } else {
+    std::vector<float2> h;
+    if ((s = load_fur(*core, fur, fur_dtype, h)) != GILA_OK) return s;
+    GILA_CUDA_TRY(cudaMemcpy(core->ker, h.data(), bytes, cudaMemcpyHostToDevice));
+  }
+  auto* o = new gila_opr;
+  o->ctx = ctx;
+  o->core = core;
+  o->trg = core->trg;
+  o->src = core->src;
+  o->adj = opt ? (opt->adj_mod != 0) : 0;
+  *out = o;
+  return GILA_OK;
+}
+
+gila_status gila_opr_fur_dims(const gila_opr* opr, int64_t dims[8][6]) {
+  if (!opr || !dims) return fail(GILA_ERR_ARG, "null argument");
+  const Core& c = *opr->core;
+  for (int eo = 0; eo < 8; ++eo) {
+    dims[eo][0] = c.geom.tru[0];
+    dims[eo][1] = c.geom.tru[1];
+    dims[eo][2] = c.geom.tru[2];
+    dims[eo][3] = 6;
+    dims[eo][4] = c.parS;
+    dims[eo][5] = c.geom.parT;
+  }
+  return GILA_OK;
+}
+
+gila_status gila_opr_export_fur(gila_opr* opr, void* const host_out[8]) {
+  if (!opr || !host_out) return fail(GILA_ERR_ARG, "null argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  GILA_CUDA_TRY(cudaSetDevice(c.device));
+  const Geom& g = c.geom;
+  const size_t cs = csize(c.dtype);
+  std::vector<unsigned char> h(c.ker_bytes);
+  GILA_CUDA_TRY(cudaMemcpy(h.data(), c.ker, c.ker_bytes, cudaMemcpyDeviceToHost));
+  const int tx = g.tru[0], ty = g.tru[1], tz = g.tru[2];
+  for (int eo = 0; eo < 8; ++eo) {
+    unsigned char* dst = static_cast<unsigned char*>(host_out[eo]);
+    if (!dst) return fail(GILA_ERR_ARG, "null output branch");
+    const int64_t n = (int64_t)tx * ty * tz * 6 * c.parS * g.parT;
+    memset(dst, 0, (size_t)n * cs);
+    for (int tp = 0; tp < g.parT; ++tp)
+      for (int cc = 0; cc < 6; ++cc)
+        for (int iz = 0; iz < tz; ++iz)
+          for (int iy = 0; iy < ty; ++iy)
+            for (int ix = 0; ix < tx; ++ix) {
+              const int64_t di = ((((int64_t)tp * c.parS) * 6 + cc) * tz + iz) * ty * (int64_t)tx + (int64_t)iy * tx + ix;
+              const int64_t si = (((((int64_t)tp * 8 + eo) * tz + iz) * ty + iy) * tx + ix) * 6 + cc;
+              memcpy(dst + di * cs, h.data() + si * cs, cs);
+            }
+  }
+  return GILA_OK;
+}
+
+gila_status gila_opr_adjoint(gila_opr* opr, gila_opr** out) {
+  if (!opr || !out) return fail(GILA_ERR_ARG, "null argument");
+  auto* o = new gila_opr;
+  o->ctx = opr->ctx;
+  o->core = opr->core;
+  o->trg = opr->src;
+  o->src = opr->trg;
+  o->adj = !opr->adj;
+  *out = o;
+  return GILA_OK;
+}
+
+gila_status gila_opr_destroy(gila_opr* opr) {
+  delete opr;
+  return GILA_OK;
+}
+
+gila_status gila_opr_sizes(const gila_opr* opr, int64_t trg[4], int64_t src[4]) {
+  if (!opr) return fail(GILA_ERR_ARG, "null operator");
+  for (int k = 0; k < 3; ++k) {
+    if (trg) trg[k] = opr->trg.cel[k];
+    if (src) src[k] = opr->src.cel[k];
+  }
+  if (trg) trg[3] = 3;
+  if (src) src[3] = 3;
+  return GILA_OK;
+}
+
+gila_status gila_opr_input_size(const gila_opr* opr, int64_t in[4]) {
+  if (!opr || !in) return fail(GILA_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; ++k) in[k] = opr->core->geom.sc[k];
+  in[3] = 3;
+  return GILA_OK;
+}
+
+gila_status gila_opr_output_size(const gila_opr* opr, int64_t o[4]) {
+  if (!opr || !o) return fail(GILA_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; ++k) o[k] = opr->core->geom.out_full[k];
+  o[3] = 3;
+  return GILA_OK;
+}
+
+gila_status gila_opr_info(const gila_opr* opr, gila_dtype* dtype, int32_t* flags) {
+  if (!opr) return fail(GILA_ERR_ARG, "null operator");
+  if (dtype) *dtype = opr->core->dtype;
+  if (flags) *flags = (vol_eq(opr->trg, opr->src) ? 1 : 0) | (opr->adj ? 2 : 0);
+  return GILA_OK;
+}
+
+gila_status gila_opr_apply(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len, void* out,
+                           int64_t out_len, int64_t nrhs, void* stream) {
+  return apply_common(opr, dtype, in, in_len, out, out_len, nrhs, false, nullptr, nullptr, stream);
+}
+
+gila_status gila_opr_apply_axpby(gila_opr* opr, gila_dtype dtype, const double alpha[2], const void* in,
+                                 int64_t in_len, const double beta[2], void* out, int64_t out_len, int64_t nrhs,
+                                 void* stream) {
+  return apply_common(opr, dtype, in, in_len, out, out_len, nrhs, true, alpha, beta, stream);
+}
+
+gila_status gila_opr_reserve(gila_opr* opr, int64_t nrhs) {
+  if (!opr) return fail(GILA_ERR_ARG, "null operator");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  GILA_CUDA_TRY(cudaSetDevice(c.device));
+  if (!c.tuned) {
+    c.launch = default_launch(c);
+    c.tuned = true;
+  }
+  return ensure_work(c, nrhs);
+}
+
+gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes) {
+  if (!opr || !bytes) return fail(GILA_ERR_ARG, "null argument");
+  const Core& c = *opr->core;
+  const Work w = work_sizes(c.geom);
+  *bytes = (int64_t)c.ker_bytes + (int64_t)(w.a_rhs + w.b_rhs) * c.cap_rhs * (int64_t)csize(c.dtype);
+  return GILA_OK;
+}
+
+gila_status gila_opr_create(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src, const gila_kopt* opt,
+                            gila_dtype dtype, gila_opr** out) {
+  (void)ctx;
+  (void)trg;
+  (void)src;
+  (void)opt;
+  (void)dtype;
+  (void)out;
+  return fail(GILA_ERR_ARG, "GPU kernel build not available in this build");
+}
+
+}  // extern "C"

@@ -1,0 +1,105 @@
+// internal.h -- host-side operator state shared by the C-ABI translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/gila_b200.h"
+#include "matvec.cuh"
+
+namespace gila {
+
+void set_error(const std::string& msg);
+gila_status fail(gila_status s, const std::string& msg);
+gila_status cuda_fail(cudaError_t e, const char* where);
+
+#define GILA_CUDA_TRY(expr)                                     \
+  do {                                                          \
+    cudaError_t e__ = (expr);                                   \
+    if (e__ != cudaSuccess) return ::gila::cuda_fail(e__, #expr); \
+  } while (0)
+
+// Rational arithmetic on int64 num/den pairs (GlaVol uses Julia Rationals).
+struct Rat {
+  int64_t n, d;
+};
+Rat rat(int64_t n, int64_t d);
+bool rat_eq(Rat a, Rat b);
+
+// Volume in rational form (GlaVol, src/glaMem.jl:12-19).
+struct Vol {
+  int64_t cel[3];
+  Rat scl[3], org[3], grd[3];
+};
+Vol vol_from_abi(const gila_vol& v);
+gila_vol vol_to_abi(const Vol& v);
+bool vol_eq(const Vol& a, const Vol& b);
+Vol vol_even(const Vol& v);
+
+struct ExtInf {  // GlaExtInf (src/glaMem.jl:39-47)
+  Rat min_scl[3];
+  int tdiv[3], sdiv[3];
+  int tc[3], sc[3];
+};
+gila_status ext_inf(const Vol& trg, const Vol& src, ExtInf* out);
+
+struct Ctx;
+
+// Device-resident operator data, shared between an operator and its adjoint.
+struct Core {
+  Ctx* ctx = nullptr;
+  int device = 0;
+  gila_dtype dtype = GILA_C128;
+  bool self = true;
+  Vol trg{}, src{};  // volumes after even-cell regeneration
+  ExtInf mix{};
+  gila_kopt opt{};
+  Geom geom{};
+  int parS = 1;
+  AxisPlan plan[3]{};
+  void* ker = nullptr;  // device, [parT][8][tz][ty][tx][6] complex
+  size_t ker_bytes = 0;
+  int* maps[3] = {nullptr, nullptr, nullptr};
+  const void* tw[3] = {nullptr, nullptr, nullptr};  // owned by ctx cache
+  // workspaces
+  void* A = nullptr;
+  void* B = nullptr;
+  int64_t cap_rhs = 0;
+  void* stage_in = nullptr;
+  void* stage_out = nullptr;
+  int64_t stage_cap_in = 0, stage_cap_out = 0;
+  Launch launch{};
+  bool tuned = false;
+  cudaStream_t stream = nullptr;
+  std::mutex mu;
+  ~Core();
+};
+
+struct Ctx {
+  int device = 0;
+  std::mutex mu;
+  std::map<std::pair<int, int>, void*> tw_cache;  // (P, dtype) -> table
+  std::map<std::string, Launch> tune_cache;
+  ~Ctx();
+};
+
+size_t csize(gila_dtype t);
+gila_status plan_axis(int P, AxisPlan* pl);
+gila_status twiddle_table(Ctx* ctx, int P, gila_dtype dt, const void** out);
+
+}  // namespace gila
+
+struct gila_ctx {
+  gila::Ctx* impl;
+};
+
+struct gila_opr {
+  gila_ctx* ctx;
+  std::shared_ptr<gila::Core> core;
+  gila::Vol trg, src;  // as reported by glaSze (swapped for the adjoint)
+  int adj;
+};

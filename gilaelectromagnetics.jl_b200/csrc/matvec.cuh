@@ -1,0 +1,77 @@
+// matvec.cuh -- geometry of one Green-operator matvec and the launchers of its
+// five passes.  See matvec.cu for the kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "fft.cuh"
+
+namespace gila {
+
+// Everything the passes need to know about one operator.  Sizes follow
+// GlaExtInf (src/glaMem.jl:39-47): sc / tc are srcCel / trgCel (cells of one
+// partition), P = sc + tc is the circulant length per axis, tru the stored
+// kernel extent per axis (src/glaMemSup.jl:121-136).
+struct Geom {
+  int sc[3];
+  int tc[3];
+  int P[3];
+  int tru[3];
+  int parT;   // target partitions (source partitions are rejected, see gila.cu)
+  int tdiv[3];
+  int toff[64][3];  // target partition offsets (x fastest), parT <= 64
+  int64_t out_full[3];  // full target volume (tc * tdiv)
+};
+
+// Workspace layout per right-hand side (complex elements):
+//   A : [3][zA][yA][Px]   zA*yA = max(sc_z*sc_y, tc_z*tc_y*parT)
+//   B : [3*maxch][Py][Px] planes, maxch = max(sc_z, tc_z*parT)
+struct Work {
+  int64_t a_rhs;  // elements of A per rhs
+  int64_t b_rhs;  // elements of B per rhs
+  int zb;         // z planes per component in B (max(sc_z, tc_z*parT))
+};
+
+Work work_sizes(const Geom& g);
+
+// Per-axis plan (radix list), twiddle tables and kernel-address maps live on
+// the device; Dev bundles the pointers for one dtype.
+template <typename C>
+struct DevOp {
+  const C* ker;      // [parT][8][tz][ty][tx][6]
+  const int* map[3]; // per axis, per frequency f: m | p<<29 | mirrored<<30
+  const C* tw[3];    // P-point twiddle tables
+  AxisPlan plan[3];
+  double scale;      // 1 / (Px Py Pz)
+};
+
+// Tile / launch parameters picked by the autotuner.
+struct Launch {
+  int xf_lines;  // lines per CTA, x forward
+  int xi_lines;  // lines per CTA, x inverse
+  int y_tx;      // kx tile, y passes
+  int z_tx;      // kx tile, z pass
+};
+
+template <typename C>
+cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A, C* B,
+                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st);
+
+// Individual passes (exposed for the autotuner and the profiler).
+template <typename C>
+cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* A, int nrhs,
+                        cudaStream_t st);
+template <typename C>
+cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int nrhs,
+                     cudaStream_t st);
+template <typename C>
+cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st);
+template <typename C>
+cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int nrhs, bool axpby,
+                        C alpha, C beta, cudaStream_t st);
+
+int smem_optin_bytes();
+// Threads per CTA of a pass over M lines of an axis plan.
+int pass_threads(const AxisPlan& pl, int M);
+
+}  // namespace gila

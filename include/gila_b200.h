@@ -1,0 +1,159 @@
+/*
+ * gila_b200.h -- C ABI of libgila_b200, a B200 (sm_100a) implementation of the
+ * discrete 3-D electromagnetic Green-operator matvec of GilaElectromagnetics.jl
+ * (v1.0.3) and of the Fourier-kernel build it consumes.
+ *
+ * Every entry point below replaces one piece of the reference's Julia API; the
+ * reference file:line of that piece is cited beside it.  A Julia shim
+ * (gilaelectromagnetics.jl_b200/julia/GilaB200.jl) keeps the reference
+ * signatures (GlaOprMem, GlaOpr, egoOpr!, mul!, *, adjoint, glaSze, size,
+ * eltype, isadjoint, isselfoperator, isexternaloperator) and swaps their
+ * bodies for ccalls into this library.
+ *
+ * Conventions
+ *  - Vectors are (Nx, Ny, Nz, 3[, nrhs]) column-major (x fastest), complex
+ *    interleaved (re, im): double2 for GILA_C128 (ComplexF64), float2 for
+ *    GILA_C64 (ComplexF32).  Multi-RHS batches are contiguous, one vector after
+ *    the other.
+ *  - Pointers may be host or device memory; the library tells them apart with
+ *    cudaPointerGetAttributes.  Host buffers are staged through pinned memory.
+ *  - No call aborts; every call returns a gila_status.  gila_last_error()
+ *    returns a message for the last failure on the calling thread.
+ *  - Calls that take a `stream` (a cudaStream_t; NULL = the operator's own
+ *    stream) enqueue work and, for host pointers or stream == NULL, wait for
+ *    it before returning.
+ */
+#ifndef GILA_B200_H
+#define GILA_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+  GILA_OK = 0,
+  GILA_ERR_ARG = 1,       /* invalid argument / unsupported option          */
+  GILA_ERR_SIZE = 2,      /* egoOpr! size check (src/glaAct.jl:37-45)       */
+  GILA_ERR_TYPE = 3,      /* element type mismatch (src/glaLinAlg.jl:35)    */
+  GILA_ERR_CUDA = 4,      /* CUDA runtime error                              */
+  GILA_ERR_NOMEM = 5,     /* device / host allocation failed                 */
+  GILA_ERR_NAN = 6,       /* non-numeric kernel (src/glaMemSup.jl:93,110,160)*/
+  GILA_ERR_NODEV = 7,     /* no usable CUDA device (src/glaMemSup.jl:22-24)  */
+  GILA_ERR_OVERLAP = 8,   /* overlapping volumes (src/glaGen.jl:77-79)       */
+  GILA_ERR_SCALE = 9,     /* no common scale grid (src/glaMem.jl:192-209)    */
+  GILA_ERR_NOTCONV = 10,  /* iterative solve hit its iteration cap           */
+  GILA_ERR_TIMEOUT = 11,  /* a bounded device-side wait ran out              */
+  GILA_ERR_INTERNAL = 12
+} gila_status;
+
+typedef enum {
+  GILA_C64 = 0,  /* ComplexF32 */
+  GILA_C128 = 1  /* ComplexF64 */
+} gila_dtype;
+
+/* GlaVol (src/glaMem.jl:12-19, constructor :136-148).  Rationals are
+ * num/den pairs.  grd = cell pitch (equals scl unless partitioned). */
+typedef struct {
+  int64_t cel[3];
+  int64_t scl_num[3], scl_den[3];
+  int64_t org_num[3], org_den[3];
+  int64_t grd_num[3], grd_den[3];
+} gila_vol;
+
+/* GlaKerOpt (src/glaMem.jl:62-70, defaults :226-233).  num_trd / num_blk are
+ * accepted for ABI compatibility and ignored: launch shapes are chosen by the
+ * library's autotuner. */
+typedef struct {
+  double frq_re, frq_im; /* frqPhz */
+  int32_t int_ord;       /* intOrd, Gauss-Legendre order of singular terms */
+  int32_t adj_mod;       /* adjMod */
+  int32_t dev_mod;       /* devMod (must be 1: this library is the device path) */
+  int32_t num_trd[3];
+  int32_t num_blk[3];
+} gila_kopt;
+
+typedef struct gila_ctx gila_ctx;
+typedef struct gila_opr gila_opr;
+
+/* ---- context --------------------------------------------------------- */
+/* One context per device: streams, twiddle tables, autotune cache.  Replaces
+ * the CUDA.functional() gate of GlaOprMem (src/glaMemSup.jl:22-24). */
+gila_status gila_ctx_create(int device, gila_ctx** out);
+gila_status gila_ctx_destroy(gila_ctx* ctx);
+const char* gila_last_error(void);
+const char* gila_status_string(gila_status s);
+/* Library version, e.g. "0.1.0". */
+const char* gila_version(void);
+
+/* ---- operator construction -------------------------------------------- */
+/* GlaOprMem(cmpInf, trgVol, srcVol=nothing; setTyp) with egoFur == nothing
+ * (src/glaMemSup.jl:16-171): builds the real-space circulant on the GPU in
+ * FP64 (src/glaGen.jl, src/glaInt.jl, src/glaIntSup.jl), FFTs it in FP64,
+ * extracts the 8 parity branches, casts to dtype.  src == NULL (or src equal
+ * to trg) gives the self operator. */
+gila_status gila_opr_create(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src,
+                            const gila_kopt* opt, gila_dtype dtype, gila_opr** out);
+
+/* GlaOprMem(...; egoFur = fur) (src/glaMemSup.jl:16-20, :158-171): accept the
+ * reference's egoFur layout.  fur[eo] (eo = 4*px + 2*py + pz) is a
+ * (tx, ty, tz, 6, parSrc, parTrg) column-major complex array of fur_dtype,
+ * component order (xx, yy, zz, xy, xz, yz), frequency 2k+p on each axis.
+ * fur_dims[eo] gives its 6 extents.  Pointers may be host or device. */
+gila_status gila_opr_create_from_fur(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src,
+                                     const gila_kopt* opt, gila_dtype dtype,
+                                     const void* const fur[8], const int64_t fur_dims[8][6],
+                                     gila_dtype fur_dtype, gila_opr** out);
+
+/* Copy the operator's egoFur back out in the reference layout (host
+ * pointers, each sized per gila_opr_fur_dims), in the operator's dtype. */
+gila_status gila_opr_fur_dims(const gila_opr* opr, int64_t dims[8][6]);
+gila_status gila_opr_export_fur(gila_opr* opr, void* const host_out[8]);
+
+/* adjoint(opr) (src/glaLinAlg.jl:16-29): a new handle that shares the
+ * operator's device memory, with adjMod flipped and the volumes swapped.  As
+ * in the reference, the matvec itself ignores adjMod. */
+gila_status gila_opr_adjoint(gila_opr* opr, gila_opr** out);
+gila_status gila_opr_destroy(gila_opr* opr);
+
+/* ---- queries ---------------------------------------------------------- */
+/* glaSze (src/glaMemSup.jl:359-371): trg = (trgVol.cel..., 3),
+ * src = (srcVol.cel..., 3). */
+gila_status gila_opr_sizes(const gila_opr* opr, int64_t trg[4], int64_t src[4]);
+/* Input size egoOpr! accepts: (mixInf.srcCel..., 3) (src/glaAct.jl:37). */
+gila_status gila_opr_input_size(const gila_opr* opr, int64_t in[4]);
+gila_status gila_opr_output_size(const gila_opr* opr, int64_t out[4]);
+/* flags: bit0 self operator, bit1 adjMod. */
+gila_status gila_opr_info(const gila_opr* opr, gila_dtype* dtype, int32_t* flags);
+
+/* ---- the hot path ------------------------------------------------------ */
+/* egoOpr!(egoMem, actVec) (src/glaAct.jl:33-49) for nrhs vectors at once:
+ * out = G * in.  `in` is not modified (the reference consumes its input;
+ * callers must not rely on either behaviour).  in_len / out_len are element
+ * counts (complex) of the buffers and are checked against the operator's
+ * input and output sizes times nrhs (GILA_ERR_SIZE, as egoOpr!'s error).
+ * `dtype` must match the operator (GILA_ERR_TYPE, as the eltype assertion of
+ * src/glaLinAlg.jl:35). */
+gila_status gila_opr_apply(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len,
+                           void* out, int64_t out_len, int64_t nrhs, void* stream);
+
+/* LinearAlgebra.mul!(out, G, in, alpha, beta) (src/glaLinAlg.jl:61-69):
+ * out = alpha * (G * in) + beta * out, with the axpby fused into the last
+ * pass.  alpha/beta are (re, im) pairs. */
+gila_status gila_opr_apply_axpby(gila_opr* opr, gila_dtype dtype, const double alpha[2],
+                                 const void* in, int64_t in_len, const double beta[2],
+                                 void* out, int64_t out_len, int64_t nrhs, void* stream);
+
+/* Pre-size the operator's workspaces for nrhs vectors (so a later apply
+ * allocates nothing) and pick launch shapes with the autotuner. */
+gila_status gila_opr_reserve(gila_opr* opr, int64_t nrhs);
+
+/* Device bytes the operator holds (kernel + workspaces). */
+gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GILA_B200_H */

@@ -1,0 +1,119 @@
+"""GPU parity of the matvec against the FP64 CPU oracle (egoBrnHst!
+restatement), through the C-ABI.
+
+Tolerances (relative L2 over the whole output): ComplexF64 <= 1e-12,
+ComplexF32 <= 1e-5.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from conftest import TOL_F32, TOL_F64, load_pkg, rel_l2
+from oracle.matvec import OprMem, ego_opr
+from oracle.synth import seeded_current, synth_operator
+
+pytestmark = pytest.mark.gpu
+
+SCL = ("1/32", "1/32", "1/32")
+
+# (trg_cel, src_cel, trg_org, src_org): self when src_cel is None
+CASES = [
+    ((8, 8, 8), None, (0, 0, 0), None),
+    ((5, 3, 6), None, (0, 0, 0), None),
+    ((2, 2, 2), None, (0, 0, 0), None),
+    ((1, 3, 2), None, (0, 0, 0), None),
+    ((16, 12, 10), None, (0, 0, 0), None),
+    ((7, 9, 5), None, (0, 0, 0), None),
+    ((4, 4, 4), (4, 4, 4), (0, "4/32", 0), (0, 0, 0)),
+    ((4, 4, 2), (6, 4, 4), ("9/32", 0, 0), (0, 0, 0)),
+    ((3, 4, 5), (5, 4, 3), ("1/2", "1/3", "1/4"), (0, 0, 0)),
+    ((8, 8, 4), (8, 8, 8), ("10/32", 0, 0), (0, 0, 0)),
+]
+
+
+def _build(gila, case, dtype):
+    tc, sc, to, so = case
+    mix, fur, crc, is_self, trg, src = synth_operator(tc, SCL, to, sc, so, set_dtype=np.complex128)
+    tv = gila.GlaVol(trg.cel, trg.scl, trg.org)
+    sv = None if is_self else gila.GlaVol(src.cel, src.scl, src.org)
+    mem = gila.GlaOprMem(gila.GlaKerOpt(True), tv, sv, egoFur=[f.astype(dtype) for f in fur], setTyp=dtype)
+    return mix, fur, mem
+
+
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}<-{c[1]}")
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_matvec_parity(case, dtype):
+    gila = load_pkg()
+    mix, fur, mem = _build(gila, case, dtype)
+    x = seeded_current(mix.src_cel, 7)
+    xin = np.asfortranarray(x.astype(dtype))
+    y = gila.egoOpr(mem, xin)
+    # oracle on the same (possibly rounded) kernel, in FP64
+    ref = ego_opr(OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur]), xin.astype(np.complex128))
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    assert rel_l2(y, ref) <= tol
+    # input untouched
+    assert np.array_equal(xin, np.asfortranarray(x.astype(dtype)))
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_multi_rhs_and_axpby(dtype):
+    gila = load_pkg()
+    mix, fur, mem = _build(gila, ((6, 10, 8), None, (0, 0, 0), None), dtype)
+    n = 5
+    xs = [seeded_current(mix.src_cel, 100 + k).astype(dtype) for k in range(n)]
+    X = np.stack([np.asfortranarray(x) for x in xs], axis=-1)
+    X = np.asfortranarray(X)
+    Y = np.empty_like(X)
+    mem.apply_into(X, Y, nrhs=n)
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    om = OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur])
+    for k in range(n):
+        assert rel_l2(Y[..., k], ego_opr(om, xs[k].astype(np.complex128))) <= tol
+    # mul!(out, G, x, alpha, beta)
+    a, b = 0.5 - 2j, 1.5 + 0.25j
+    out0 = np.asfortranarray(seeded_current(mix.trg_cel, 3).astype(dtype))
+    out = out0.copy(order="F")
+    G = gila.GlaOpr(mem)
+    gila.mul(out, G, xs[0], a, b)
+    ref = a * ego_opr(om, xs[0].astype(np.complex128)) + b * out0.astype(np.complex128)
+    assert rel_l2(out, ref) <= tol
+
+
+def test_device_tensors_and_determinism():
+    import torch
+    gila = load_pkg()
+    mix, fur, mem = _build(gila, ((12, 8, 10), None, (0, 0, 0), None), np.complex128)
+    x = seeded_current(mix.src_cel, 11)
+    xt = torch.from_numpy(np.ascontiguousarray(x.transpose(3, 2, 1, 0))).cuda()
+    y1 = gila.egoOpr(mem, xt)
+    y2 = gila.egoOpr(mem, xt)
+    torch.cuda.synchronize()
+    assert torch.equal(y1, y2)  # bit-identical on repeat
+    ref = ego_opr(OprMem(mix, fur), x)
+    got = y1.cpu().numpy().transpose(3, 2, 1, 0)
+    assert rel_l2(got, ref) <= TOL_F64
+
+
+def test_self_external_identity():
+    """test/extSlfTest.jl:44-47: G_U(x_A) restricted to B equals
+    G_ext(B<-A)(x_A) for A, B touching halves of U."""
+    gila = load_pkg()
+    celA = (8, 8, 8)
+    celU = (8, 16, 8)
+    scl = ("1/50", "1/50", "1/50")
+    # U centred at 0 spans y in [-8,8)/50; A = lower half centred at -4/50,
+    # B = upper half centred at +4/50
+    mixU, furU, _, _, trgU, _ = synth_operator(celU, scl, (0, 0, 0))
+    mixE, furE, _, _, trgB, srcA = synth_operator(celA, scl, (0, "4/50", 0), celA, (0, "-4/50", 0))
+    opt = gila.GlaKerOpt(True)
+    memU = gila.GlaOprMem(opt, gila.GlaVol(celU, scl, (0, 0, 0)), egoFur=furU)
+    memE = gila.GlaOprMem(opt, gila.GlaVol(celA, scl, (0, "4/50", 0)), gila.GlaVol(celA, scl, (0, "-4/50", 0)),
+                          egoFur=furE)
+    xU = np.zeros((*celU, 3), dtype=np.complex128, order="F")
+    xA = seeded_current(celA, 5)
+    xU[:, :8, :, :] = xA
+    yU = gila.egoOpr(memU, xU)
+    yE = gila.egoOpr(memE, np.asfortranarray(xA))
+    assert rel_l2(yE, yU[:, 8:, :, :]) <= 1e-12
