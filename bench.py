@@ -1,0 +1,397 @@
+#!/usr/bin/env python
+"""Benchmark of the Green-operator matvec (egoOpr!) on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+One step = one application of the ComplexF64 self Green operator to one
+source current on the 128x128x64-cell volume with 1/32-wavelength cells (the
+matvec precision sweep configuration; its ComplexF32 leg, the external
+64^3 -> 64x64x32 operator and the 256x256x128 roofline target are reported
+in "sweep").  Inputs are seeded i.i.d. complex N(0,1) currents and a seeded
+synthetic Fourier kernel with the reference's storage shapes (kernel values do
+not change the matvec's work).  Under torchrun each rank runs an independent
+replica on its own GPU (weak scaling); `value` is the whole-job matvec/s from
+the max over ranks of the device time.
+
+Prints one JSON line (rank 0).
+"""
+from __future__ import annotations
+
+import argparse
+import importlib.util
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = os.path.join(ROOT, "gilaelectromagnetics.jl_b200")
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = "Green matvec/s (ComplexF64 egoOpr!, self 128x128x64)"
+CEL = (128, 128, 64)
+SCL = ("1/32", "1/32", "1/32")
+L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
+
+
+def load_pkg():
+    if "gila_b200" in sys.modules:
+        return sys.modules["gila_b200"]
+    spec = importlib.util.spec_from_file_location("gila_b200", os.path.join(PKG, "__init__.py"),
+                                                  submodule_search_locations=[PKG])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["gila_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def tru_self(cel):
+    """Stored kernel extent per axis of a self operator (src/glaMemSup.jl:121-136)."""
+    return [max((n + 1) // 2 + (1 if n % 2 == 0 else 0), 2) for n in cel]
+
+
+def synthetic_fur(tru, dtype, seed):
+    rng = np.random.default_rng(seed)
+    return [np.asfortranarray((rng.standard_normal((*tru, 6, 1, 1))
+                               + 1j * rng.standard_normal((*tru, 6, 1, 1))).astype(dtype)) for _ in range(8)]
+
+
+def tmin_bytes(src, trg, tru, csize):
+    """Algorithmic bytes of one matvec, 3-pass model: read x, write+read the
+    x,y-padded spectrum, read the kernel, write+read the z-truncated spectrum,
+    write y."""
+    Px, Py = src[0] + trg[0], src[1] + trg[1]
+    Ns, Nt = math.prod(src), math.prod(trg)
+    K = 8 * math.prod(tru)
+    return csize * (3 * Ns + 6 * Px * Py * src[2] + 6 * K + 6 * Px * Py * trg[2] + 3 * Nt)
+
+
+def zpass_bytes(src, trg, tru, csize):
+    """Algorithmic bytes of one z-pass launch (the dominant kernel): read the
+    x,y spectrum (3 components, source z planes), read the stored kernel,
+    write the z-truncated spectrum."""
+    Px, Py = src[0] + trg[0], src[1] + trg[1]
+    K = 8 * math.prod(tru)
+    return csize * (3 * Px * Py * src[2] + 6 * K + 3 * Px * Py * trg[2])
+
+
+class Clocks:
+    """nvidia-smi sampler (200 ms) around the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                                       "-i", str(index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except Exception:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        with open(self.f.name) as fh:
+            for line in fh:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) >= 9:
+                    rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def ncu_traffic(key):
+    """Per-launch DRAM bytes of the dominant kernel from the committed ncu
+    summary (profiles/traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            return json.load(f).get(key)
+    except Exception:
+        return None
+
+
+def make_opr(gila, cel, dtype, seed=1, src_cel=None, trg_org=(0, 0, 0), src_org=(0, 0, 0)):
+    if src_cel is None:
+        tru = tru_self(cel)
+        fur = synthetic_fur(tru, dtype, seed)
+        mem = gila.GlaOprMem(gila.GlaKerOpt(True), gila.GlaVol(cel, SCL), egoFur=fur, setTyp=dtype)
+        return mem, tru
+    # external operator: full storage along axes whose cells / centres differ
+    tru = []
+    for d in range(3):
+        if cel[d] == src_cel[d] and trg_org[d] == src_org[d]:
+            tru.append(tru_self((cel[d],))[0])
+        else:
+            tru.append((cel[d] + src_cel[d]) // 2)
+    fur = synthetic_fur(tru, dtype, seed)
+    mem = gila.GlaOprMem(gila.GlaKerOpt(True), gila.GlaVol(cel, SCL, trg_org), gila.GlaVol(src_cel, SCL, src_org),
+                         egoFur=fur, setTyp=dtype)
+    return mem, tru
+
+
+def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, seed=3):
+    """matvec/s with device-resident vectors; per-step CUDA events, L2
+    flushed between steps (outside the events)."""
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    x = torch.randn((3, cel_in[2], cel_in[1], cel_in[0]), dtype=tdt, device="cuda", generator=g)
+    y = torch.empty((3, cel_out[2], cel_out[1], cel_out[0]), dtype=tdt, device="cuda")
+    sp = stream.cuda_stream
+    for _ in range(warmup):
+        mem.apply_into(x, y, stream=sp)
+    torch.cuda.synchronize()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    with torch.cuda.stream(stream):
+        for k in range(steps):
+            flush.zero_()
+            ev[k][0].record(stream)
+            mem.apply_into(x, y, stream=sp)
+            ev[k][1].record(stream)
+    torch.cuda.synchronize()
+    ms = sum(a.elapsed_time(b) for a, b in ev)
+    return ms, y
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-sweep", action="store_true")
+    a = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if a.impl == "reference":
+        if rank != 0:
+            return 0
+        return run_reference(a, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    gila = load_pkg()
+    gila.default_context(local)
+
+    mem, tru = make_opr(gila, CEL, np.complex128)
+    mem.reserve(1)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.Stream()
+    W = max(a.warmup, 3)
+
+    # ---- value: device-resident inputs
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clk = Clocks(local)
+    ms, y_dev = device_rate(torch, mem, CEL, CEL, torch.complex128, a.steps, W, stream, flush)
+    clocks = clk.stop()
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = world * a.steps / (ms_max / 1e3)
+
+    # ---- e2e: public API with pinned host buffers, copies inside the timed region
+    xh = torch.randn((3, CEL[2], CEL[1], CEL[0]), dtype=torch.complex128).pin_memory()
+    yh = torch.empty_like(xh).pin_memory()
+    sp = stream.cuda_stream
+    for _ in range(W):
+        mem.apply_into(xh, yh, stream=sp)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(a.steps):
+        # host buffers: the call copies H2D, runs the passes, copies D2H and
+        # waits, all on `stream`, so the events bracket the whole device timeline
+        mem.apply_into(xh, yh, stream=sp)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_value = world * a.steps / (float(t.item()) / 1e3)
+    nbytes = xh.numel() * xh.element_size()
+
+    # ---- roofline of the dominant kernel (z pass), timed live
+    passes = mem.time_passes(1, reps=max(3, min(a.steps, 10)))
+    zb = zpass_bytes(CEL, CEL, tru, 16)
+    peak, peak_kind = measured_peak()
+    achieved = zb / (passes[1] / 1e3) / 1e9
+    traffic = ncu_traffic("z_pass_c128_128x128x64")
+    roofline = {"bound": "hbm", "kernel": "k_z_ct (z pencils: FFT, 3x3 multiply, inverse FFT)",
+                "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
+                "frac": round(achieved / peak, 4), "traffic": traffic,
+                "algorithmic_bytes_per_launch": zb, "launch_ms": round(passes[1], 4),
+                "pass_ms": {"xy_fwd": round(passes[0], 4), "z": round(passes[1], 4), "yx_inv": round(passes[2], 4)},
+                "matvec_tmin_bytes": tmin_bytes(CEL, CEL, tru, 16),
+                "matvec_tmin_frac": round(tmin_bytes(CEL, CEL, tru, 16) / (ms_max / a.steps / 1e3) / 1e9 / peak, 4)}
+
+    out = {
+        "metric": METRIC, "value": round(value, 2), "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
+        "warmup": W, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "complex128 (f64)",
+        "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
+        "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, ComplexF64, 1 vector/step",
+                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
+        "e2e": {"value": round(e2e_value, 2), "unit": "matvec/s", "h2d_bytes_per_step": nbytes,
+                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors"},
+        "gpu_launches": int(mem.launches_per_apply(1)) * a.steps,
+        "roofline": roofline,
+        "clocks": clocks,
+    }
+
+    if rank == 0 and world == 1:
+        out["cpu_baseline"] = cpu_baseline()
+    if not a.no_sweep and world == 1:
+        out["sweep"] = sweep(torch, gila, stream, flush, y_dev)
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    return 0
+
+
+def sweep(torch, gila, stream, flush, y64):
+    """F32 leg, external operator and the 256x256x128 roofline target."""
+    res = {}
+    peak, _ = measured_peak()
+    # F32 self 128x128x64 and its error against the F64 GPU result
+    mem32, tru = make_opr(gila, CEL, np.complex64)
+    ms, _ = device_rate(torch, mem32, CEL, CEL, torch.complex64, 10, 3, stream, flush)
+    g = torch.Generator(device="cuda").manual_seed(3)
+    x64 = torch.randn((3, CEL[2], CEL[1], CEL[0]), dtype=torch.complex128, device="cuda", generator=g)
+    res["self_128x128x64_c64"] = {"ms": round(ms / 10, 4), "matvec_per_s": round(1e4 / ms, 2),
+                                  "tmin_frac": round(tmin_bytes(CEL, CEL, tru, 8) / (ms / 10 / 1e3) / 1e9 / peak, 4)}
+    del mem32
+    # external 64^3 -> 64x64x32, target offset 80 cells along x
+    for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
+        src, trg = (64, 64, 64), (64, 64, 32)
+        mem, tru = make_opr(gila, trg, dt, src_cel=src, trg_org=("80/32", 0, 0))
+        ms, _ = device_rate(torch, mem, src, trg, tdt, 10, 3, stream, flush)
+        res[f"external_64cube_to_64x64x32_{np.dtype(dt).name}"] = {
+            "ms": round(ms / 10, 4), "matvec_per_s": round(1e4 / ms, 2),
+            "tmin_frac": round(tmin_bytes(src, trg, tru, cs) / (ms / 10 / 1e3) / 1e9 / peak, 4)}
+        del mem
+    # 256x256x128 (north-star roofline target)
+    big = (256, 256, 128)
+    for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
+        mem, tru = make_opr(gila, big, dt)
+        ms, _ = device_rate(torch, mem, big, big, tdt, 5, 3, stream, flush)
+        tm = tmin_bytes(big, big, tru, cs)
+        res[f"self_256x256x128_{np.dtype(dt).name}"] = {
+            "ms": round(ms / 5, 4), "matvec_per_s": round(5e3 / ms, 2), "tmin_bytes": tm,
+            "tmin_frac": round(tm / (ms / 5 / 1e3) / 1e9 / peak, 4)}
+        del mem
+    torch.cuda.empty_cache()
+    return res
+
+
+def cpu_baseline():
+    """The oracle's restatement of the reference host path (egoBrnHst!) with
+    scipy.fft on all host threads, on the same configuration: a bounded
+    sample of 2 matvecs."""
+    from oracle.gla_mem import ExtInf, Vol
+    from oracle.matvec import OprMem, ego_opr, use_fft_workers
+    n = os.cpu_count() or 1
+    use_fft_workers(n)
+    v = Vol.make(CEL, SCL)
+    mix = ExtInf.make(v, v)
+    fur = synthetic_fur(tru_self(CEL), np.complex128, 1)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((*CEL, 3)) + 1j * rng.standard_normal((*CEL, 3))
+    om = OprMem(mix, fur)
+    ego_opr(om, x)  # warm-up
+    reps = 2
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        ego_opr(om, x)
+    dt = time.perf_counter() - t0
+    return {"value": round(reps / dt, 4), "unit": "matvec/s", "cores": n, "kind": "port",
+            "sample": f"{reps} matvecs of the same 128x128x64 ComplexF64 self operator (numpy/scipy.fft "
+                      f"restatement of egoBrnHst!, FFT workers={n}, elementwise steps single-threaded)"}
+
+
+def run_reference(a, world):
+    """--impl reference: the reference's CPU path (egoBrnHst!, restated in
+    the oracle; the Julia package cannot run on this image) on all host
+    threads, same configuration and metric."""
+    from oracle.gla_mem import ExtInf, Vol
+    from oracle.matvec import OprMem, ego_opr, use_fft_workers
+    n = os.cpu_count() or 1
+    use_fft_workers(n)
+    v = Vol.make(CEL, SCL)
+    mix = ExtInf.make(v, v)
+    fur = synthetic_fur(tru_self(CEL), np.complex128, 1)
+    rng = np.random.default_rng(3)
+    x = rng.standard_normal((*CEL, 3)) + 1j * rng.standard_normal((*CEL, 3))
+    om = OprMem(mix, fur)
+    t0 = time.perf_counter()
+    for _ in range(max(1, min(a.warmup, 2))):
+        ego_opr(om, x)
+    per = (time.perf_counter() - t0) / max(1, min(a.warmup, 2))
+    budget = 150.0
+    k = max(1, min(a.steps, int(budget / max(per, 1e-3))))
+    t0 = time.perf_counter()
+    for _ in range(k):
+        ego_opr(om, x)
+    dt = time.perf_counter() - t0
+    val = k / dt
+    sample = (f"{k} of {a.steps} requested steps timed (1 matvec each; the rest skipped to bound the CPU run), "
+              f"numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n}")
+    out = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "matvec/s", "n_gpus": world,
+           "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / k * 1e3, 2), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
+           "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel",
+           "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, ComplexF64, 1 vector/step",
+                      "parallelism": "host threads"},
+           "cpu_baseline": {"value": round(val, 4), "unit": "matvec/s", "cores": n, "kind": "port", "sample": sample},
+           "e2e": {"value": round(val, 4), "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

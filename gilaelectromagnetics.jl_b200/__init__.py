@@ -319,6 +319,17 @@ class GlaOprMem:
     def reserve(self, nrhs: int):
         _check(L.lib().gila_opr_reserve(self._h, int(nrhs)))
 
+    def time_passes(self, nrhs: int = 1, reps: int = 5):
+        """Device ms of one apply: (forward x/y, z pass, inverse y/x, total)."""
+        ms = (ct.c_double * 4)()
+        _check(L.lib().gila_opr_time_passes(self._h, int(nrhs), int(reps), ms))
+        return tuple(ms)
+
+    def launches_per_apply(self, nrhs: int = 1) -> int:
+        n = ct.c_int64()
+        _check(L.lib().gila_opr_launches_per_apply(self._h, int(nrhs), ct.byref(n)))
+        return n.value
+
     def device_bytes(self) -> int:
         v = ct.c_int64()
         _check(L.lib().gila_opr_device_bytes(self._h, ct.byref(v)))

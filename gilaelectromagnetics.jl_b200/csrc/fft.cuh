@@ -164,7 +164,64 @@ template <bool INV, typename C> struct Bfly<7, INV, C> {
   }
 };
 
+// ------------------------------------------------------------ async copy
+// Global -> shared copies that bypass registers (cp.async), so that a CTA
+// can put its whole input tile in flight at once.
+__device__ __forceinline__ void cp_async(double2* s, const double2* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async(float2* s, const float2* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// -------------------------------------------------------- fast division
+// n / d for 0 <= n < 2^31 by multiply-high and shift (Granlund-Montgomery);
+// the magic numbers are computed once on the host.
+struct FDiv {
+  uint32_t d, m, s;
+  __host__ __device__ __forceinline__ uint32_t div(uint32_t n) const { return (__umulhi_hd(n, m) + n) >> s; }
+  __host__ __device__ __forceinline__ static uint32_t __umulhi_hd(uint32_t a, uint32_t b) {
+#ifdef __CUDA_ARCH__
+    return __umulhi(a, b);
+#else
+    return (uint32_t)(((uint64_t)a * b) >> 32);
+#endif
+  }
+};
+
+inline FDiv make_fdiv(uint32_t d) {
+  FDiv f;
+  f.d = d;
+  uint32_t s = 0;
+  while ((1ull << s) < d) ++s;
+  f.s = s;
+  f.m = (uint32_t)((((1ull << s) - d) << 32) / d + 1);
+  if (d == 1) f.m = 0;
+  return f;
+}
+
 // ------------------------------------------------------------- one stage
+// Per-stage constants of a Stockham plan, precomputed on the host.
+struct StageC {
+  int R;      // radix
+  int ns;     // span Ns = product of the previous radices
+  int tpl;    // tasks per line = P / R
+  int twst;   // twiddle stride P / (Ns * R)
+  FDiv nsd;   // division by Ns
+  FDiv tpld;  // division by tpl
+};
+
+// A plan for one axis: the radix of each stage (product = P).
+struct AxisPlan {
+  int P;
+  int nst;
+  int radix[12];
+  StageC st[12];
+};
+
 // Stockham autosort stage of radix R and span Ns over M lines of length P.
 // Task (l, j), j in [0, P/R), reads positions j + r*P/R of line l, applies
 // the twiddles w_P^{r*(j mod Ns)*P/(Ns*R)}, runs the R-point butterfly and
@@ -173,10 +230,10 @@ template <bool INV, typename C> struct Bfly<7, INV, C> {
 // in-place shared-memory stage the caller passes sync_mid = true so that all
 // loads complete before any store.  E = complex values staged per thread.
 template <typename C, int R, int E, bool INV, bool LINE_FAST, class Ld, class St>
-__device__ __forceinline__ void fft_stage(int M, int P, int Ns, const C* __restrict__ tw, const Ld& ld,
-                                          const St& st, bool sync_mid) {
+__device__ __forceinline__ void fft_stage(int M, const FDiv& md, const StageC& sc, const C* __restrict__ tw,
+                                          const Ld& ld, const St& st, bool sync_mid) {
   constexpr int K = (E + R - 1) / R;  // K*R >= E covers every task
-  const int tpl = P / R;
+  const int tpl = sc.tpl;
   const int ntask = M * tpl;
   C v[K][R];
   int tl[K], tj[K];
@@ -188,10 +245,10 @@ __device__ __forceinline__ void fft_stage(int M, int P, int Ns, const C* __restr
     if (task < ntask) {
       int l, j;
       if (LINE_FAST) {
-        l = task % M;
-        j = task / M;
+        j = (int)md.div((uint32_t)task);
+        l = task - j * M;
       } else {
-        l = task / tpl;
+        l = (int)sc.tpld.div((uint32_t)task);
         j = task - l * tpl;
       }
       tl[k] = l;
@@ -205,13 +262,14 @@ __device__ __forceinline__ void fft_stage(int M, int P, int Ns, const C* __restr
   for (int k = 0; k < K; ++k) {
     if (tl[k] >= 0) {
       const int j = tj[k];
-      const int jm = j % Ns;
+      const int Ns = sc.ns;
+      const int jm = j - (int)sc.nsd.div((uint32_t)j) * Ns;
       if (Ns > 1) {
-        const int step = jm * (P / (Ns * R));
+        const int step = jm * sc.twst;
 #pragma unroll
         for (int r = 1; r < R; ++r) v[k][r] = cmul(v[k][r], twid<INV>(tw, r * step));
       }
-      Bfly<R, INV, C>::run(v[k], tw, P / R);
+      Bfly<R, INV, C>::run(v[k], tw, tpl);
       const int base = (j - jm) * R + jm;
 #pragma unroll
       for (int r = 0; r < R; ++r) st(tl[k], base + r * Ns, v[k][r]);
@@ -219,24 +277,38 @@ __device__ __forceinline__ void fft_stage(int M, int P, int Ns, const C* __restr
   }
 }
 
-// A plan for one axis: the radix of each stage (product = P).
-struct AxisPlan {
-  int P;
-  int nst;
-  int radix[12];
-};
-
 // Run all stages of a plan.  The first stage reads through ld_first, the last
 // writes through st_last; intermediate stages work in place on shared memory
-// through ld_mid / st_mid.  A __syncthreads() separates stages.
+// through ld_mid / st_mid.  A __syncthreads() separates stages.  md divides
+// by the line count M (used when lines are the fastest-varying task index).
+__device__ __forceinline__ StageC load_stage(const AxisPlan* __restrict__ pl, int s) {
+  const StageC* q = pl->st + s;
+  StageC c;
+  c.R = __ldg(&q->R);
+  c.ns = __ldg(&q->ns);
+  c.tpl = __ldg(&q->tpl);
+  c.twst = __ldg(&q->twst);
+  c.nsd.d = __ldg(&q->nsd.d);
+  c.nsd.m = __ldg(&q->nsd.m);
+  c.nsd.s = __ldg(&q->nsd.s);
+  c.tpld.d = __ldg(&q->tpld.d);
+  c.tpld.m = __ldg(&q->tpld.m);
+  c.tpld.s = __ldg(&q->tpld.s);
+  return c;
+}
+
+// The plan lives in device memory (read through the read-only cache): a
+// kernel-parameter copy indexed by the runtime stage number would be spilled
+// to per-thread local memory.
 template <typename C, int E, bool INV, bool LINE_FAST, bool MIXED, class LdF, class LdM, class StM, class StL>
-__device__ __forceinline__ void fft_run(const AxisPlan& pl, int M, const C* __restrict__ tw, const LdF& ld_first,
-                                        const LdM& ld_mid, const StM& st_mid, const StL& st_last,
-                                        bool first_in_smem, bool last_in_smem) {
-  int Ns = 1;
-  for (int s = 0; s < pl.nst; ++s) {
-    const int R = pl.radix[s];
-    const bool first = (s == 0), last = (s == pl.nst - 1);
+__device__ __forceinline__ void fft_run(const AxisPlan* __restrict__ pl, int M, const FDiv& md,
+                                        const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
+                                        const StM& st_mid, const StL& st_last, bool first_in_smem,
+                                        bool last_in_smem) {
+  const int nst = __ldg(&pl->nst);
+  for (int s = 0; s < nst; ++s) {
+    const StageC sc = load_stage(pl, s);
+    const bool first = (s == 0), last = (s == nst - 1);
     // in-place hazard only when both source and destination are shared memory
     const bool sync_mid = (first ? first_in_smem : true) && (last ? last_in_smem : true);
     auto ld = [&](int l, int i) { return first ? ld_first(l, i) : ld_mid(l, i); };
@@ -246,19 +318,18 @@ __device__ __forceinline__ void fft_run(const AxisPlan& pl, int M, const C* __re
       else
         st_mid(l, i, v);
     };
-    switch (R) {
-      case 8: fft_stage<C, 8, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid); break;
-      case 4: fft_stage<C, 4, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid); break;
-      case 2: fft_stage<C, 2, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid); break;
+    switch (sc.R) {
+      case 8: fft_stage<C, 8, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid); break;
+      case 4: fft_stage<C, 4, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid); break;
+      case 2: fft_stage<C, 2, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid); break;
       default:
         if constexpr (MIXED) {
-          if (R == 3) fft_stage<C, 3, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid);
-          else if (R == 5) fft_stage<C, 5, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid);
-          else if (R == 7) fft_stage<C, 7, E, INV, LINE_FAST>(M, pl.P, Ns, tw, ld, st, sync_mid);
+          if (sc.R == 3) fft_stage<C, 3, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid);
+          else if (sc.R == 5) fft_stage<C, 5, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid);
+          else if (sc.R == 7) fft_stage<C, 7, E, INV, LINE_FAST>(M, md, sc, tw, ld, st, sync_mid);
         }
         break;
     }
-    Ns *= R;
     __syncthreads();
   }
 }

@@ -1,0 +1,170 @@
+// fft_ct.cuh -- compile-time specialised Stockham stages.
+//
+// Same algorithm as fft_run in fft.cuh, but the transform length, the radix
+// schedule, the span of every stage and the line count are template
+// constants, so all index arithmetic folds to shifts / immediates and every
+// stage is unrolled.  Used for the circulant lengths the workloads use; other
+// lengths run the runtime-sized path.
+#pragma once
+#include "fft.cuh"
+
+namespace gila {
+
+// greedy radix schedule: 8s, then a 4 or a 2, then 3s, 5s, 7s
+constexpr int ct_pow2(int P) {
+  int t = 0;
+  while (P % 2 == 0) {
+    P /= 2;
+    ++t;
+  }
+  return t;
+}
+constexpr int ct_odd(int P) {
+  while (P % 2 == 0) P /= 2;
+  return P;
+}
+constexpr int ct_nst(int P) {
+  int t = ct_pow2(P);
+  int n = t / 3 + ((t % 3) ? 1 : 0);
+  int o = ct_odd(P);
+  for (int q : {3, 5, 7})
+    while (o % q == 0) {
+      o /= q;
+      ++n;
+    }
+  return n;
+}
+constexpr int ct_radix(int P, int s) {
+  int t = ct_pow2(P);
+  int n8 = t / 3;
+  if (s < n8) return 8;
+  s -= n8;
+  if (t % 3) {
+    if (s == 0) return (t % 3 == 2) ? 4 : 2;
+    --s;
+  }
+  int o = ct_odd(P);
+  for (int q : {3, 5, 7})
+    while (o % q == 0) {
+      if (s == 0) return q;
+      o /= q;
+      --s;
+    }
+  return 1;
+}
+constexpr int ct_span(int P, int s) {
+  int ns = 1;
+  for (int k = 0; k < s; ++k) ns *= ct_radix(P, k);
+  return ns;
+}
+constexpr bool ct_supported(int P) { return ct_odd(P) == 1 || ct_odd(P) == 3 || ct_odd(P) == 5 || ct_odd(P) == 9; }
+
+// One stage; T = threads per CTA, M = lines.
+template <typename C, int P, int S, int E, int T, int M, bool INV, bool LINE_FAST, class Ld, class St>
+__device__ __forceinline__ void ct_stage(const C* __restrict__ tw, const Ld& ld, const St& st, bool sync_mid) {
+  constexpr int R = ct_radix(P, S);
+  constexpr int NS = ct_span(P, S);
+  constexpr int TPL = P / R;
+  constexpr int NTASK = M * TPL;
+  constexpr int K = (NTASK + T - 1) / T;
+  constexpr int TWST = P / (NS * R);
+  C v[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NTASK % T == 0 || task < NTASK) {
+      int l, j;
+      if (LINE_FAST) {
+        l = task % M;
+        j = task / M;
+      } else {
+        l = task / TPL;
+        j = task % TPL;
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[k][r] = ld(l, j + r * TPL);
+    }
+  }
+  if (sync_mid) __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NTASK % T == 0 || task < NTASK) {
+      int l, j;
+      if (LINE_FAST) {
+        l = task % M;
+        j = task / M;
+      } else {
+        l = task / TPL;
+        j = task % TPL;
+      }
+      const int jm = j % NS;
+      if (NS > 1) {
+        const int step = jm * TWST;
+#pragma unroll
+        for (int r = 1; r < R; ++r) v[k][r] = cmul(v[k][r], twid<INV>(tw, r * step));
+      }
+      Bfly<R, INV, C>::run(v[k], tw, TPL);
+      const int base = (j - jm) * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r) st(l, base + r * NS, v[k][r]);
+    }
+  }
+}
+
+template <typename C, int P, int S, int E, int T, int M, bool INV, bool LINE_FAST, class LdF, class LdM, class StM,
+          class StL>
+__device__ __forceinline__ void ct_run_from(const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
+                                            const StM& st_mid, const StL& st_last, bool first_in_smem,
+                                            bool last_in_smem) {
+  if constexpr (S < ct_nst(P)) {
+    constexpr bool first = (S == 0), last = (S == ct_nst(P) - 1);
+    const bool sync_mid = (first ? first_in_smem : true) && (last ? last_in_smem : true);
+    if constexpr (first && last)
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_first, st_last, sync_mid);
+    else if constexpr (first)
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_first, st_mid, sync_mid);
+    else if constexpr (last)
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_mid, st_last, sync_mid);
+    else
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_mid, st_mid, sync_mid);
+    __syncthreads();
+    ct_run_from<C, P, S + 1, E, T, M, INV, LINE_FAST>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem,
+                                                      last_in_smem);
+  }
+}
+
+template <typename C, int P, int E, int T, int M, bool INV, bool LINE_FAST, class LdF, class LdM, class StM, class StL>
+__device__ __forceinline__ void ct_run(const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
+                                       const StM& st_mid, const StL& st_last, bool first_in_smem, bool last_in_smem) {
+  ct_run_from<C, P, 0, E, T, M, INV, LINE_FAST>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem, last_in_smem);
+}
+
+// ---------------------------------------------------------- launch shapes
+// Shared by the kernels (template constants) and the host (launch config).
+constexpr int ct_round32(int a) { return (a + 31) / 32 * 32; }
+// rows per CTA of an x pass
+template <int CS>
+constexpr int ct_xlines(int P) {
+  return P >= 2048 ? 1 : 2048 / P;
+}
+// kx tile of a y pass: 128-byte rows, at most 512 threads with E = 8
+template <int CS>
+constexpr int ct_ytile(int P) {
+  int tx = 128 / CS;
+  while (tx > 1 && ct_round32((tx * P + 7) / 8) > 512) tx /= 2;
+  return tx;
+}
+// kx tile of the z pass: three components in shared memory (<= 100 KB)
+template <int CS>
+constexpr int ct_ztile(int P) {
+  int tx = 128 / CS;
+  while (tx > 1 && (ct_round32((tx * P + 7) / 8) > 512 || 3 * tx * P * CS > 100 * 1024)) tx /= 2;
+  return tx;
+}
+constexpr int ct_threads(int M, int P) {
+  int t = ct_round32((M * P + 7) / 8);
+  return t < 32 ? 32 : t;
+}
+
+}  // namespace gila

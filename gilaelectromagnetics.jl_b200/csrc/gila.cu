@@ -6,6 +6,7 @@
 #include <cmath>
 #include <complex>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 #include <string>
@@ -153,6 +154,17 @@ gila_status plan_axis(int P, AxisPlan* pl) {
     return fail(GILA_ERR_ARG, "circulant length " + std::to_string(P) +
                                   " has a prime factor above 7; supported lengths are 2^a 3^b 5^c 7^d");
   if (pl->nst == 0) pl->radix[pl->nst++] = 2;  // P == 1 cannot occur (P even)
+  int ns = 1;
+  for (int s = 0; s < pl->nst; ++s) {
+    StageC& c = pl->st[s];
+    c.R = pl->radix[s];
+    c.ns = ns;
+    c.tpl = P / c.R;
+    c.twst = P / (ns * c.R);
+    c.nsd = make_fdiv((uint32_t)ns);
+    c.tpld = make_fdiv((uint32_t)c.tpl);
+    ns *= c.R;
+  }
   return GILA_OK;
 }
 
@@ -197,6 +209,7 @@ Core::~Core() {
   if (stream) cudaStreamSynchronize(stream);
   cudaFree(ker);
   for (int k = 0; k < 3; ++k) cudaFree(maps[k]);
+  cudaFree(plan_d);
   cudaFree(A);
   cudaFree(B);
   cudaFree(stage_in);
@@ -292,6 +305,14 @@ static gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_
   int parT = core->mix.tdiv[0] * core->mix.tdiv[1] * core->mix.tdiv[2];
   if (parT > 64) return fail(GILA_ERR_ARG, "more than 64 target partitions are not supported");
   g.parT = parT;
+  g.csize = (int)csize(dtype);
+  g.max_rhs = 1;
+  // GILA_SLAB_BYTES overrides the x/y slab size (tuning and tests)
+  g.slab_bytes = kSlabBytes;
+  if (const char* e = getenv("GILA_SLAB_BYTES")) {
+    const long v = atol(e);
+    if (v > 0) g.slab_bytes = (int)v;
+  }
   for (int k = 0; k < 3; ++k) {
     g.sc[k] = core->mix.sc[k];
     g.tc[k] = core->mix.tc[k];
@@ -315,6 +336,8 @@ static gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_
     GILA_CUDA_TRY(cudaMalloc(&core->maps[k], m.size() * sizeof(int)));
     GILA_CUDA_TRY(cudaMemcpy(core->maps[k], m.data(), m.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
+  GILA_CUDA_TRY(cudaMalloc(&core->plan_d, 3 * sizeof(AxisPlan)));
+  GILA_CUDA_TRY(cudaMemcpy(core->plan_d, core->plan, 3 * sizeof(AxisPlan), cudaMemcpyHostToDevice));
   GILA_CUDA_TRY(cudaStreamCreateWithFlags(&core->stream, cudaStreamNonBlocking));
   return GILA_OK;
 }
@@ -386,6 +409,7 @@ static DevOp<C> devop(const Core& c) {
     d.map[k] = c.maps[k];
     d.tw[k] = static_cast<const C*>(c.tw[k]);
     d.plan[k] = c.plan[k];
+    d.plan_d[k] = c.plan_d + k;
   }
   d.scale = 1.0 / ((double)c.geom.P[0] * c.geom.P[1] * c.geom.P[2]);
   return d;
@@ -397,35 +421,42 @@ static Launch default_launch(const Core& c) {
   const Geom& g = c.geom;
   const int cs = (int)csize(c.dtype);
   Launch L;
-  auto lines = [&](int P) {
-    int m = 2048 / P;
+  auto lines = [&](const AxisPlan& pl) {
+    int m = 2048 / pl.P;
     if (m < 1) m = 1;
-    while (m > 1 && ((m * P + 7) / 8 > 512)) --m;
+    while (m > 1 && pass_threads(pl, m) > 512) --m;
     return m;
   };
-  L.xf_lines = lines(g.P[0]);
-  L.xi_lines = lines(g.P[0]);
-  auto tile = [&](int P, int ch, int want, int smem_budget) {
+  L.xf_lines = lines(c.plan[0]);
+  L.xi_lines = lines(c.plan[0]);
+  auto tile = [&](const AxisPlan& pl, int ch, int want, int smem_budget) {
     int tx = want;
-    while (tx > 1 && (((ch * tx * P + 7) / 8) > 512 || (int64_t)ch * tx * P * cs > smem_budget)) tx /= 2;
-    if (tx > g.P[0]) tx = g.P[0];
+    while (tx > 1 && (pass_threads(pl, ch * tx) > 512 || (int64_t)ch * tx * pl.P * cs > smem_budget)) tx /= 2;
     return tx < 1 ? 1 : tx;
   };
   const int want = c.dtype == GILA_C128 ? 8 : 16;
-  L.y_tx = tile(g.P[1], 1, want, 96 * 1024);
-  L.z_tx = tile(g.P[2], 3 * (g.parT > 1 ? 2 : 1), want, 110 * 1024);
+  L.y_tx = tile(c.plan[1], 1, want, 96 * 1024);
+  // the z pass runs its FFTs one component at a time (threads for TX lines)
+  // but keeps all three components' spectra in shared memory
+  {
+    int tx = want;
+    const int64_t budget = (g.parT > 1 ? 55 : 110) * 1024;
+    while (tx > 1 && (pass_threads(c.plan[2], tx) > 512 || 3LL * tx * c.plan[2].P * cs > budget)) tx /= 2;
+    L.z_tx = tx < 1 ? 1 : tx;
+  }
   return L;
 }
 
 static gila_status ensure_work(Core& c, int64_t nrhs) {
   if (nrhs <= c.cap_rhs) return GILA_OK;
+  c.geom.max_rhs = (int)nrhs;
   const Work w = work_sizes(c.geom);
   const size_t cs = csize(c.dtype);
   cudaFree(c.A);
   cudaFree(c.B);
   c.A = c.B = nullptr;
   c.cap_rhs = 0;
-  GILA_CUDA_TRY(cudaMalloc(&c.A, (size_t)(w.a_rhs * nrhs) * cs));
+  GILA_CUDA_TRY(cudaMalloc(&c.A, (size_t)w.a_elems * cs));
   GILA_CUDA_TRY(cudaMalloc(&c.B, (size_t)(w.b_rhs * nrhs) * cs));
   c.cap_rhs = nrhs;
   return GILA_OK;
@@ -449,6 +480,9 @@ static gila_status apply_t(Core& c, const void* in, void* out, int64_t nrhs, boo
   }
   cudaStream_t st = user_st ? user_st : c.stream;
   const bool din = is_device_ptr(in), dout = is_device_ptr(out);
+  // element alignment (the passes copy with 16 / 8 byte cp.async)
+  if ((din && ((uintptr_t)in % cs)) || (dout && ((uintptr_t)out % cs)))
+    return fail(GILA_ERR_ARG, "device vectors must be aligned to their complex element size");
   const C* d_in = static_cast<const C*>(in);
   C* d_out = static_cast<C*>(out);
   if (!din) {
@@ -504,6 +538,56 @@ static gila_status apply_common(gila_opr* opr, gila_dtype dtype, const void* in,
   if (c.dtype == GILA_C128)
     return apply_t<double2>(c, in, out, nrhs, axpby, alpha, beta, static_cast<cudaStream_t>(stream));
   return apply_t<float2>(c, in, out, nrhs, axpby, alpha, beta, static_cast<cudaStream_t>(stream));
+}
+
+template <typename C>
+gila_status time_passes_t(Core& c, int64_t nrhs, int reps, double ms[4]) {
+  gila_status s = ensure_work(c, nrhs);
+  if (s != GILA_OK) return s;
+  if (!c.tuned) {
+    c.launch = default_launch(c);
+    c.tuned = true;
+  }
+  const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
+  C *din = nullptr, *dout = nullptr;
+  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
+  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
+  if (e != cudaSuccess) {
+    cudaFree(din);
+    return cuda_fail(e, "cudaMalloc");
+  }
+  cudaMemsetAsync(din, 0, (size_t)ni * sizeof(C), c.stream);
+  cudaEvent_t ev[4];
+  for (auto& x : ev) cudaEventCreate(&x);
+  double acc[3] = {0, 0, 0};
+  const DevOp<C> d = devop<C>(c);
+  C one, zero;
+  one.x = 1;
+  one.y = 0;
+  zero.x = 0;
+  zero.y = 0;
+  for (int r = -1; r < reps && e == cudaSuccess; ++r) {
+    cudaEventRecord(ev[0], c.stream);
+    for (int ph = 0; ph < 3 && e == cudaSuccess; ++ph) {
+      e = launch_matvec_phase<C>(ph, c.geom, d, c.launch, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B),
+                                 (int)nrhs, false, one, zero, c.stream);
+      cudaEventRecord(ev[ph + 1], c.stream);
+    }
+    cudaEventSynchronize(ev[3]);
+    if (r >= 0)  // r = -1 is a warm-up
+      for (int ph = 0; ph < 3; ++ph) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[ph], ev[ph + 1]);
+        acc[ph] += t;
+      }
+  }
+  for (auto& x : ev) cudaEventDestroy(x);
+  cudaFree(din);
+  cudaFree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "time_passes");
+  for (int ph = 0; ph < 3; ++ph) ms[ph] = acc[ph] / reps;
+  ms[3] = ms[0] + ms[1] + ms[2];
+  return GILA_OK;
 }
 
 }  // namespace gila
@@ -719,8 +803,25 @@ gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes) {
   if (!opr || !bytes) return fail(GILA_ERR_ARG, "null argument");
   const Core& c = *opr->core;
   const Work w = work_sizes(c.geom);
-  *bytes = (int64_t)c.ker_bytes + (int64_t)(w.a_rhs + w.b_rhs) * c.cap_rhs * (int64_t)csize(c.dtype);
+  *bytes = (int64_t)c.ker_bytes + (w.a_elems + w.b_rhs * c.cap_rhs) * (int64_t)csize(c.dtype);
   return GILA_OK;
+}
+
+gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n) {
+  if (!opr || !n || nrhs < 1) return fail(GILA_ERR_ARG, "invalid argument");
+  Geom g = opr->core->geom;
+  if (nrhs > g.max_rhs) g.max_rhs = (int)nrhs;
+  *n = matvec_launches(g, (int)nrhs);
+  return GILA_OK;
+}
+
+gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double ms[4]) {
+  if (!opr || !ms || nrhs < 1 || reps < 1) return fail(GILA_ERR_ARG, "invalid argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  GILA_CUDA_TRY(cudaSetDevice(c.device));
+  if (c.dtype == GILA_C128) return time_passes_t<double2>(c, nrhs, reps, ms);
+  return time_passes_t<float2>(c, nrhs, reps, ms);
 }
 
 gila_status gila_opr_create(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src, const gila_kopt* opt,

@@ -64,6 +64,7 @@ struct Core {
   void* ker = nullptr;  // device, [parT][8][tz][ty][tx][6] complex
   size_t ker_bytes = 0;
   int* maps[3] = {nullptr, nullptr, nullptr};
+  AxisPlan* plan_d = nullptr;  // device copies of plan[3]
   const void* tw[3] = {nullptr, nullptr, nullptr};  // owned by ctx cache
   // workspaces
   void* A = nullptr;

@@ -21,17 +21,26 @@ struct Geom {
   int tdiv[3];
   int toff[64][3];  // target partition offsets (x fastest), parT <= 64
   int64_t out_full[3];  // full target volume (tc * tdiv)
+  int csize;            // bytes per complex element
+  int slab_bytes;       // target size of the x/y slab buffer
+  int max_rhs;          // right-hand sides the workspaces are sized for
 };
 
-// Workspace layout per right-hand side (complex elements):
-//   A : [3][zA][yA][Px]   zA*yA = max(sc_z*sc_y, tc_z*tc_y*parT)
-//   B : [3*maxch][Py][Px] planes, maxch = max(sc_z, tc_z*parT)
+// Workspaces (complex elements):
+//   A : one slab of slab_planes planes (ch, z) of max(sy, ty) rows of Px,
+//       shared by all rhs (the x and y passes run slab by slab)
+//   B : per rhs [3*zb][Py][Px] planes, zb = max(sc_z, tc_z*parT)
 struct Work {
-  int64_t a_rhs;  // elements of A per rhs
-  int64_t b_rhs;  // elements of B per rhs
-  int zb;         // z planes per component in B (max(sc_z, tc_z*parT))
+  int64_t slab_planes;  // planes per slab
+  int64_t a_elems;      // elements of the slab buffer A
+  int64_t b_rhs;        // elements of B per rhs
+  int zb;               // z planes per component in B
 };
 
+// Default slab size.  Slabs small enough to stay L2-resident between the x
+// and y passes cut HBM traffic but multiply the launch count; the default
+// keeps one slab (whole volume) until the launches are graph-captured.
+constexpr int kSlabBytes = 1 << 30;
 Work work_sizes(const Geom& g);
 
 // Per-axis plan (radix list), twiddle tables and kernel-address maps live on
@@ -41,7 +50,8 @@ struct DevOp {
   const C* ker;      // [parT][8][tz][ty][tx][6]
   const int* map[3]; // per axis, per frequency f: m | p<<29 | mirrored<<30
   const C* tw[3];    // P-point twiddle tables
-  AxisPlan plan[3];
+  AxisPlan plan[3];          // host copies (launch decisions)
+  const AxisPlan* plan_d[3]; // device copies (read by the kernels)
   double scale;      // 1 / (Px Py Pz)
 };
 
@@ -59,18 +69,27 @@ cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, con
 
 // Individual passes (exposed for the autotuner and the profiler).
 template <typename C>
-cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* A, int nrhs,
+cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* A, int64_t rows,
                         cudaStream_t st);
 template <typename C>
-cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int nrhs,
-                     cudaStream_t st);
+cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int64_t q0,
+                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st);
 template <typename C>
 cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st);
 template <typename C>
-cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int nrhs, bool axpby,
-                        C alpha, C beta, cudaStream_t st);
+cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int64_t rows,
+                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st);
 
 int smem_optin_bytes();
+
+// Kernels one matvec of nrhs vectors launches.
+int64_t matvec_launches(const Geom& g, int nrhs);
+
+// The three phases of launch_matvec, for timing: forward x/y slabs, z pass,
+// inverse y/x slabs.
+template <typename C>
+cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out,
+                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st);
 // Threads per CTA of a pass over M lines of an axis plan.
 int pass_threads(const AxisPlan& pl, int M);
 

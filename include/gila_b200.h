@@ -152,6 +152,16 @@ gila_status gila_opr_reserve(gila_opr* opr, int64_t nrhs);
 /* Device bytes the operator holds (kernel + workspaces). */
 gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes);
 
+/* Profiling (no counterpart in the reference, which has no timers beyond
+ * @time in the examples): device time of one apply on nrhs device-resident
+ * vectors, averaged over `reps`, measured with CUDA events on the operator's
+ * stream.  ms[0] = forward x/y passes, ms[1] = z pass (FFT, 3x3 multiply,
+ * inverse FFT), ms[2] = inverse y/x passes, ms[3] = whole apply. */
+gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double ms[4]);
+
+/* Number of kernels one apply of nrhs vectors launches. */
+gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,6 +29,20 @@ import numpy as np
 from .gla_mem import ExtInf
 
 
+_fft = np.fft.fft
+_ifft = np.fft.ifft
+
+
+def use_fft_workers(n: int) -> None:
+    """Run the 1-D transforms with scipy.fft on n threads (the reference runs
+    FFTW with FFTW.set_num_threads(nthreads()), test/preamble.jl:1-14); the
+    elementwise split / merge / multiply steps stay single-threaded numpy."""
+    global _fft, _ifft
+    import scipy.fft as sfft
+    _fft = lambda a, axis: sfft.fft(a, axis=axis, workers=n)  # noqa: E731
+    _ifft = lambda a, axis: sfft.ifft(a, axis=axis, workers=n)  # noqa: E731
+
+
 class OprMem:
     """The parts of GlaOprMem (src/glaMem.jl:93-104) that egoOpr! reads."""
 
@@ -206,7 +220,7 @@ def _brn(mem: OprMem, lvl: int, bid: int, act: np.ndarray) -> np.ndarray:
     else:
         org = act
     if lvl > 0:
-        org = np.fft.fft(org, axis=lvl - 1).astype(mem.dtype, copy=False)
+        org = _fft(org, axis=lvl - 1).astype(mem.dtype, copy=False)
     if lvl < 3:
         ax = lvl
         if org.shape[ax] == brn[ax]:
@@ -240,7 +254,7 @@ def _brn(mem: OprMem, lvl: int, bid: int, act: np.ndarray) -> np.ndarray:
                 _mul_brn(mix, bid, ret[..., t], mem.fur[bid][:, :, :, :, s_, t],
                          org[..., s_], brn)
     if lvl > 0:
-        ret = np.fft.ifft(ret, axis=lvl - 1).astype(mem.dtype, copy=False)
+        ret = _ifft(ret, axis=lvl - 1).astype(mem.dtype, copy=False)
     if lvl == 0:
         if par_t == 1:
             return ret.reshape(*mix.trg_cel, 3)

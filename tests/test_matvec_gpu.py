@@ -117,3 +117,22 @@ def test_self_external_identity():
     yU = gila.egoOpr(memU, xU)
     yE = gila.egoOpr(memE, np.asfortranarray(xA))
     assert rel_l2(yE, yU[:, 8:, :, :]) <= 1e-12
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_multi_slab_path(dtype, monkeypatch):
+    """x/y passes split into many L2 slabs (tiny slab size) and several rhs,
+    on a non-cubic external operator."""
+    monkeypatch.setenv("GILA_SLAB_BYTES", "2048")
+    gila = load_pkg()
+    case = ((8, 6, 4), (6, 10, 8), ("13/32", 0, 0), (0, 0, 0))
+    mix, fur, mem = _build(gila, case, dtype)
+    n = 3
+    xs = [seeded_current(mix.src_cel, 40 + k).astype(dtype) for k in range(n)]
+    X = np.asfortranarray(np.stack(xs, axis=-1))
+    Y = np.empty((*mix.trg_cel, 3, n), dtype=dtype, order="F")
+    mem.apply_into(X, Y, nrhs=n)
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    om = OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur])
+    for k in range(n):
+        assert rel_l2(Y[..., k], ego_opr(om, xs[k].astype(np.complex128))) <= tol
