@@ -1,0 +1,196 @@
+#=
+GilaB200.jl -- drop-in device path for GilaElectromagnetics.jl's Green operator.
+
+Keeps the reference's operator API (src/glaMemSup.jl GlaOprMem / GlaOpr
+constructors, src/glaAct.jl egoOpr!, src/glaLinAlg.jl *, mul!, adjoint, size,
+eltype, glaSze and predicates) and runs every matvec in libgila_b200.so (sm_100a
+CUDA) through ccall.  The C declarations are in include/gila_b200.h.
+
+Usage (a maintainer would swap these in for the CUDA.jl device path):
+
+    using GilaElectromagnetics          # GlaVol, GlaKerOpt, glaSze, ...
+    include("GilaB200.jl"); using .GilaB200
+    mem = GilaB200.GlaOprMem(GlaKerOpt(true), GlaVol((32,32,32), (1//32,1//32,1//32), (0//1,0//1,0//1)))
+    y = GilaB200.egoOpr!(mem, x)        # x::Array{ComplexF64,4} or CuArray
+
+This file is not exercised in the build's test-suite (no Julia toolchain in
+the build image); the same entry points are tested through Python ctypes.
+=#
+module GilaB200
+
+using LinearAlgebra
+
+const LIB = get(ENV, "GILA_B200_LIB", joinpath(@__DIR__, "..", "libgila_b200.so"))
+
+# gila_status codes (include/gila_b200.h)
+const GILA_OK = Cint(0)
+const GILA_ERR_SIZE = Cint(2)
+const GILA_ERR_TYPE = Cint(3)
+const GILA_C64 = Cint(0)
+const GILA_C128 = Cint(1)
+
+struct CVol               # gila_vol
+    cel::NTuple{3,Int64}
+    scl_num::NTuple{3,Int64}; scl_den::NTuple{3,Int64}
+    org_num::NTuple{3,Int64}; org_den::NTuple{3,Int64}
+    grd_num::NTuple{3,Int64}; grd_den::NTuple{3,Int64}
+end
+
+struct CKopt              # gila_kopt
+    frq_re::Cdouble; frq_im::Cdouble
+    int_ord::Int32; adj_mod::Int32; dev_mod::Int32
+    num_trd::NTuple{3,Int32}; num_blk::NTuple{3,Int32}
+end
+
+cvol(v) = CVol(Int64.(Tuple(v.cel)),
+    Int64.(numerator.(v.scl)), Int64.(denominator.(v.scl)),
+    Int64.(numerator.(v.org)), Int64.(denominator.(v.org)),
+    Int64.(numerator.(Rational.(step.(v.grd)))), Int64.(denominator.(Rational.(step.(v.grd)))))
+
+function ckopt(o)
+    t = isempty(o.numTrd) ? (0, 0, 0) : o.numTrd
+    b = isempty(o.numBlk) ? (0, 0, 0) : o.numBlk
+    CKopt(real(o.frqPhz), imag(o.frqPhz), Int32(o.intOrd), Int32(o.adjMod), Int32(1), Int32.(t), Int32.(b))
+end
+
+dtcode(::Type{ComplexF64}) = GILA_C128
+dtcode(::Type{ComplexF32}) = GILA_C64
+dtcode(T) = throw(ArgumentError("setTyp must be a subtype of Complex"))
+
+lasterr() = unsafe_string(ccall((:gila_last_error, LIB), Cstring, ()))
+
+function check(st)
+    st == GILA_OK && return nothing
+    msg = lasterr()
+    st == GILA_ERR_TYPE && throw(AssertionError(msg))
+    error(msg)
+end
+
+const CTX = Ref{Ptr{Cvoid}}(C_NULL)
+function ctx()
+    if CTX[] == C_NULL
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:gila_ctx_create, LIB), Cint, (Cint, Ref{Ptr{Cvoid}}), 0, r))
+        CTX[] = r[]
+    end
+    CTX[]
+end
+
+"""GlaOprMem backed by libgila_b200 (src/glaMemSup.jl:16-20)."""
+mutable struct GlaOprMem{T}
+    h::Ptr{Cvoid}
+    cmpInf::Any
+    trgVol::Any
+    srcVol::Any
+    function GlaOprMem{T}(h, c, t, s) where {T}
+        m = new{T}(h, c, t, s)
+        finalizer(x -> ccall((:gila_opr_destroy, LIB), Cint, (Ptr{Cvoid},), x.h), m)
+        m
+    end
+end
+
+function GlaOprMem(cmpInf, trgVol, srcVol=nothing; egoFur=nothing, setTyp::DataType=ComplexF64)
+    code = dtcode(setTyp)
+    tv = Ref(cvol(trgVol)); o = Ref(ckopt(cmpInf))
+    sv = srcVol === nothing ? C_NULL : Ref(cvol(srcVol))
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    if egoFur === nothing
+        check(ccall((:gila_opr_create, LIB), Cint,
+            (Ptr{Cvoid}, Ref{CVol}, Ptr{CVol}, Ref{CKopt}, Cint, Ref{Ptr{Cvoid}}),
+            ctx(), tv, srcVol === nothing ? C_NULL : sv, o, code, r))
+    else
+        fur = [Array(f) for f in egoFur]                 # host copies, reference layout
+        ptrs = [pointer(f) for f in fur]
+        dims = zeros(Int64, 6, 8)
+        for e in 1:8, k in 1:6
+            dims[k, e] = size(fur[e], k)
+        end
+        GC.@preserve fur begin
+            check(ccall((:gila_opr_create_from_fur, LIB), Cint,
+                (Ptr{Cvoid}, Ref{CVol}, Ptr{CVol}, Ref{CKopt}, Cint, Ptr{Ptr{Cvoid}}, Ptr{Int64}, Cint,
+                 Ref{Ptr{Cvoid}}),
+                ctx(), tv, srcVol === nothing ? C_NULL : sv, o, code, ptrs, dims,
+                dtcode(eltype(fur[1])), r))
+        end
+    end
+    GlaOprMem{setTyp}(r[], cmpInf, trgVol, srcVol === nothing ? trgVol : srcVol)
+end
+
+"""GlaOpr wrapper (src/glaMem.jl:116-119)."""
+struct GlaOpr
+    mem::GlaOprMem
+end
+
+function GlaOpr(cel::NTuple{3,Int}, scl::NTuple{3,Rational}, org::NTuple{3,Rational}=(0//1, 0//1, 0//1);
+                useGpu::Bool=true, setTyp::DataType=ComplexF64)
+    setTyp <: Complex || throw(ArgumentError("setTyp must be a subtype of Complex"))
+    vol = (cel=cel, scl=scl, org=org, grd=[StepRange(o, s, o) for (o, s) in zip(org, scl)])
+    GlaOpr(GlaOprMem((frqPhz=1.0 + 0im, intOrd=32, adjMod=false, numTrd=(), numBlk=()), vol; setTyp=setTyp))
+end
+
+function sizes(m::GlaOprMem)
+    i = zeros(Int64, 4); o = zeros(Int64, 4)
+    check(ccall((:gila_opr_input_size, LIB), Cint, (Ptr{Cvoid}, Ptr{Int64}), m.h, i))
+    check(ccall((:gila_opr_output_size, LIB), Cint, (Ptr{Cvoid}, Ptr{Int64}), m.h, o))
+    Tuple(i), Tuple(o)
+end
+
+"""egoOpr!(egoMem, actVec) (src/glaAct.jl:33-49).  Host Arrays and CuArrays
+(any pointer the CUDA runtime can classify) are accepted; the result has the
+input's array type."""
+function egoOpr!(m::GlaOprMem{T}, actVec::AbstractArray{T}) where {T}
+    insz, outsz = sizes(m)
+    size(actVec) == insz || error("Size of input vector does not match size of source volume. " *
+                                  "Required data layout is (srcCelX, srcCelY, srcCelZ, 3).")
+    out = similar(actVec, T, outsz...)
+    check(ccall((:gila_opr_apply, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cvoid}, Int64, Ptr{Cvoid}, Int64, Int64, Ptr{Cvoid}),
+        m.h, dtcode(T), pointer(actVec), length(actVec), pointer(out), length(out), 1, C_NULL))
+    out
+end
+
+Base.eltype(o::GlaOpr) = typeof(o.mem).parameters[1]
+glaSze(o::GlaOpr) = ((Tuple(o.mem.trgVol.cel)..., 3), (Tuple(o.mem.srcVol.cel)..., 3))
+glaSze(o::GlaOpr, d::Int) = glaSze(o)[d]
+Base.size(o::GlaOpr) = (3 * prod(o.mem.trgVol.cel), 3 * prod(o.mem.srcVol.cel))
+Base.size(o::GlaOpr, d::Int) = size(o)[d]
+LinearAlgebra.issymmetric(::GlaOpr) = false
+LinearAlgebra.ishermitian(::GlaOpr) = false
+LinearAlgebra.isposdef(::GlaOpr) = false
+LinearAlgebra.isdiag(::GlaOpr) = false
+isadjoint(o::GlaOpr) = o.mem.cmpInf.adjMod
+isselfoperator(o::GlaOpr) = o.mem.srcVol == o.mem.trgVol
+isexternaloperator(o::GlaOpr) = !isselfoperator(o)
+
+function Base.adjoint(o::GlaOpr)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:gila_opr_adjoint, LIB), Cint, (Ptr{Cvoid}, Ref{Ptr{Cvoid}}), o.mem.h, r))
+    c = o.mem.cmpInf
+    c2 = merge(NamedTuple{propertynames(c)}(getproperty.(Ref(c), propertynames(c))), (adjMod=!c.adjMod,))
+    GlaOpr(GlaOprMem{eltype(o)}(r[], c2, o.mem.srcVol, o.mem.trgVol))
+end
+
+function Base.:*(o::GlaOpr, x::AbstractArray{T,4}) where {T<:Complex}
+    @assert T <: eltype(o) "Input array must have the same element type as the operator. eltype(opr) = $(eltype(o))"
+    egoOpr!(o.mem, x)              # the library never mutates its input
+end
+
+function Base.:*(o::GlaOpr, x::AbstractArray{T}) where {T<:Complex}
+    y = o * reshape(x, glaSze(o, 2))
+    length(x) == prod(glaSze(o, 1)) && return reshape(y, size(x))
+    ndims(x) == 1 && return vec(y)
+    reshape(y, glaSze(o, 1))
+end
+
+"""mul!(y, G, x, α, β) (src/glaLinAlg.jl:61-69) with the axpby fused on the GPU."""
+function LinearAlgebra.mul!(y::AbstractArray{T}, o::GlaOpr, x::AbstractArray{T}, α::Number, β::Number) where {T<:Complex}
+    @assert T <: eltype(o) "Input array must have the same element type as the operator."
+    length(x) == prod(glaSze(o, 2)) || throw(DimensionMismatch("input length"))
+    a = Cdouble[real(α), imag(α)]; b = Cdouble[real(β), imag(β)]
+    check(ccall((:gila_opr_apply_axpby, LIB), Cint,
+        (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cvoid}, Int64, Ptr{Cdouble}, Ptr{Cvoid}, Int64, Int64, Ptr{Cvoid}),
+        o.mem.h, dtcode(T), a, pointer(x), length(x), b, pointer(y), length(y), 1, C_NULL))
+    y
+end
+
+end # module
