@@ -85,6 +85,8 @@ _SIGS = [
     ("gila_opr_device_bytes", ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int64)]),
     ("gila_opr_time_passes", ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_double * 4]),
     ("gila_opr_launches_per_apply", ct.c_int, [ct.c_void_p, ct.c_int64, ct.POINTER(ct.c_int64)]),
+    ("gila_opr_apply_noalloc", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p,
+                                          ct.c_int64, ct.c_void_p]),
 ]
 
 # entry points added by later components; bound when present

@@ -417,7 +417,7 @@ static DevOp<C> devop(const Core& c) {
 
 // Launch shapes: the largest tiles whose thread count stays <= 512 with 8
 // staged values per thread and whose shared memory stays within budget.
-static Launch default_launch(const Core& c) {
+Launch default_launch(const Core& c) {
   const Geom& g = c.geom;
   const int cs = (int)csize(c.dtype);
   Launch L;

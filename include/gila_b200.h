@@ -162,6 +162,22 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 /* Number of kernels one apply of nrhs vectors launches. */
 gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n);
 
+/* A matvec that allocates no device memory.  This entry point has no
+ * counterpart in the reference.  It computes out = G * in for one vector,
+ * like gila_opr_apply, for callers that cannot let the library call
+ * cudaMalloc at apply time: code recording into a CUDA stream capture, hosts
+ * whose own memory pool owns all device memory, loops that forbid allocation
+ * after start-up.  The scratch between the passes lives in one fixed 64 MiB
+ * device array that every GPU loading the library holds until the process
+ * exits; operators whose padded spectrum does not fit are rejected with
+ * GILA_ERR_SIZE.  `in` and `out` must be device pointers (host vectors would
+ * need staging buffers).  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  All calls
+ * on a device share the array and calls that overlap on the GPU race on it.
+ * stream == NULL runs on the operator's stream and waits. */
+gila_status gila_opr_apply_noalloc(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len,
+                                   void* out, int64_t out_len, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
