@@ -136,3 +136,24 @@ def test_multi_slab_path(dtype, monkeypatch):
     om = OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur])
     for k in range(n):
         assert rel_l2(Y[..., k], ego_opr(om, xs[k].astype(np.complex128))) <= tol
+
+
+def test_golden_fixtures_gpu():
+    """The committed oracle fixtures (tests/golden) through the C ABI."""
+    import glob
+    import os
+    from fractions import Fraction
+    from conftest import ROOT
+    gila = load_pkg()
+    files = sorted(glob.glob(os.path.join(ROOT, "tests", "golden", "*.npz")))
+    assert files
+    for f in files:
+        d = np.load(f)
+        trg = gila.GlaVol(tuple(int(v) for v in d["trg_cel"]), SCL, tuple(Fraction(s) for s in d["trg_org"]))
+        src = None if bool(d["is_self"]) else gila.GlaVol(tuple(int(v) for v in d["src_cel"]), SCL,
+                                                          tuple(Fraction(s) for s in d["src_org"]))
+        for dtype, tol in ((np.complex128, TOL_F64), (np.complex64, TOL_F32)):
+            mem = gila.GlaOprMem(gila.GlaKerOpt(True), trg, src, egoFur=[d[f"fur{e}"].astype(dtype) for e in range(8)],
+                                 setTyp=dtype)
+            y = gila.egoOpr(mem, np.asfortranarray(d["x"].astype(dtype)))
+            assert rel_l2(y, d["y"]) <= tol, (f, dtype)
