@@ -103,3 +103,28 @@ def test_python_mirror_host_logic():
     # GlaOpr with a non-complex setTyp raises ArgumentError (test/oprTest.jl:4-5)
     with pytest.raises(gila.ArgumentError):
         gila.GlaOpr((1, 1, 1), ("1", "1", "1"), (0, 0, 0), setTyp=np.float64)
+
+
+def test_kernel_build_oracle_relations():
+    """C restatement of the kernel build (oracle/gen.c): the reference's
+    self-vs-external identity (test/extSlfTest.jl:44-47) with real kernels
+    (B touches A: the contact path of genEgoCrcExt!), symmetry of the 3x3
+    blocks, and Gauss-Legendre nodes."""
+    import numpy.polynomial.legendre as npl
+    from oracle import kerbuild as kb
+    x, w = kb.gauleg(32)
+    xr, wr = npl.leggauss(32)
+    assert np.abs(x - xr).max() < 1e-15 and np.abs(w - wr).max() < 1e-14
+    scl = ("1/50", "1/50", "1/50")
+    weak = kb.weak(scl, int_ord=8)
+    mixU, furU, crcU, _, _, _ = kb.build_operator((4, 8, 4), scl, int_ord=8, weak_vals=weak)
+    mixE, furE, _, is_self, _, _ = kb.build_operator((4, 4, 4), scl, (0, "2/50", 0), (4, 4, 4), (0, "-2/50", 0),
+                                                     int_ord=8)
+    assert not is_self
+    xA = seeded_current((4, 4, 4), 3)
+    xU = np.zeros((4, 8, 4, 3), dtype=np.complex128)
+    xU[:, :4] = xA
+    yU = ego_opr(OprMem(mixU, furU), xU)
+    yE = ego_opr(OprMem(mixE, furE), xA)
+    assert rel_l2(yE, yU[:, 4:]) < 1e-12
+    assert np.abs(crcU[0, 1] - crcU[1, 0]).max() < 1e-12 * np.abs(crcU[0, 1]).max()
