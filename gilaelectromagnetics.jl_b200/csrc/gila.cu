@@ -826,13 +826,21 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 
 gila_status gila_opr_create(gila_ctx* ctx, const gila_vol* trg, const gila_vol* src, const gila_kopt* opt,
                             gila_dtype dtype, gila_opr** out) {
-  (void)ctx;
-  (void)trg;
-  (void)src;
-  (void)opt;
-  (void)dtype;
-  (void)out;
-  return fail(GILA_ERR_ARG, "GPU kernel build not available in this build");
+  if (!out) return fail(GILA_ERR_ARG, "null output");
+  if (!ctx) return fail(GILA_ERR_ARG, "null context");
+  GILA_CUDA_TRY(cudaSetDevice(ctx->impl->device));
+  std::shared_ptr<Core> core;
+  gila_status s = init_core(ctx, trg, src, opt, dtype, core);
+  if (s != GILA_OK) return s;
+  if ((s = build_kernel(*core)) != GILA_OK) return s;
+  auto* o = new gila_opr;
+  o->ctx = ctx;
+  o->core = core;
+  o->trg = core->trg;
+  o->src = core->src;
+  o->adj = opt ? (opt->adj_mod != 0) : 0;
+  *out = o;
+  return GILA_OK;
 }
 
 }  // extern "C"

@@ -90,6 +90,8 @@ struct Ctx {
 
 size_t csize(gila_dtype t);
 Launch default_launch(const Core& c);
+// GPU FP64 Fourier-kernel build into c.ker (kerbuild.cu)
+gila_status build_kernel(Core& c);
 gila_status plan_axis(int P, AxisPlan* pl);
 gila_status twiddle_table(Ctx* ctx, int P, gila_dtype dt, const void** out);
 
