@@ -17,6 +17,9 @@ The names, argument meanings and error behaviour follow the reference:
   adjoint, isadjoint, isselfoperator, isexternaloperator, glaSze, size,
   eltype, issymmetric, isposdef, ishermitian, isdiag
                                                    src/glaLinAlg.jl, glaMemSup.jl:359-371
+  LippmannSchwinger(G, medium), ls * x, mul(y, ls, x)
+                                                   examples/GilaOperators.jl:57-96
+  solve(ls, i)               BiCGStab(l) solve     examples/scattering_film.jl:58-61
 
 Vectors use the reference's memory layout: (Nx, Ny, Nz, 3) column-major.
 numpy arrays are passed as shape (Nx, Ny, Nz, 3) in Fortran order (or flat);
@@ -38,7 +41,7 @@ __all__ = [
     "GlaVol", "GlaKerOpt", "GlaOprMem", "GlaOpr", "egoOpr", "mul", "adjoint", "isadjoint",
     "isselfoperator", "isexternaloperator", "glaSze", "size", "eltype", "issymmetric",
     "isposdef", "ishermitian", "isdiag", "GilaError", "DimensionMismatch", "ArgumentError",
-    "Context", "default_context",
+    "Context", "default_context", "cast", "LippmannSchwinger", "solve", "SolveInfo",
 ]
 
 
@@ -537,3 +540,153 @@ def mul(outVec, opr: GlaOpr, innVec, alpha=1.0, beta=0.0):
     else:
         opr.mem.axpby_into(alpha, innVec, beta, o)
     return outVec
+
+
+def cast(opr: GlaOpr, setTyp) -> GlaOpr:
+    """The same operator in another precision (the Fourier kernel cast on the
+    device); used to pair a ComplexF64 operator with its ComplexF32 copy."""
+    h = ct.c_void_p()
+    _check(L.lib().gila_opr_cast(opr.mem._h, _dtype_code(setTyp), ct.byref(h)))
+    m = opr.mem
+    return GlaOpr(GlaOprMem._from_handle(h, m.ctx, m.cmpInf, m.trgVol, m.srcVol))
+
+
+class LippmannSchwinger:
+    """LippmannSchwinger(greens_op, medium) (examples/GilaOperators.jl:57-82):
+    the operator x -> x - medium .* (G x), medium per cell broadcast over the
+    three components.  `medium` has the target cell shape (Nx, Ny, Nz)."""
+
+    def __init__(self, greens_op: GlaOpr, medium):
+        cel = tuple(greens_op.glaSze(1)[:3])
+        med = medium
+        if _is_torch(med):
+            shp = tuple(med.shape)
+            if shp not in (cel, (cel[2], cel[1], cel[0])):
+                raise DimensionMismatch("Green's operator and medium must have the same size.")
+            med = med.detach().cpu().numpy()
+            if shp == (cel[2], cel[1], cel[0]):
+                med = np.ascontiguousarray(med).reshape(-1).reshape(cel, order="F")
+        else:
+            med = np.asarray(med)
+            if tuple(med.shape) != cel:
+                raise DimensionMismatch("Green's operator and medium must have the same size.")
+        if np.dtype(med.dtype) != np.dtype(greens_op.dtype):
+            raise ArgumentError("Medium must have the same element type as the Green's operator.")
+        self.greens_op = greens_op
+        self.medium = np.asfortranarray(med)
+        self._g32 = None
+
+    def glaSze(self, dim: Optional[int] = None):
+        return self.greens_op.glaSze(dim)
+
+    def size(self, dim: Optional[int] = None):
+        return self.greens_op.size(dim)
+
+    @property
+    def dtype(self):
+        return self.greens_op.dtype
+
+    def _mul(self, x):
+        """ls * x = x - medium .* (G x) (examples/GilaOperators.jl:89-95)."""
+        gx = self.greens_op * x
+        if _is_torch(x):
+            import torch
+            cel = self.glaSze(1)[:3]
+            chi = torch.from_numpy(np.ascontiguousarray(self.medium.reshape(-1, order="F"))).to(x.device)
+            chi = chi.reshape(cel[2], cel[1], cel[0])
+            return x - (chi * gx.reshape(3, cel[2], cel[1], cel[0])).reshape(x.shape)
+        xa = np.asarray(x)
+        cel = self.glaSze(1)[:3]
+        g4 = np.reshape(gx, (*cel, 3), order="F")
+        return xa - np.reshape(self.medium[..., None] * g4, xa.shape, order="F")
+
+    def __mul__(self, x):
+        return self._mul(x)
+
+    def __matmul__(self, x):
+        return self._mul(x)
+
+    def g32(self) -> GlaOpr:
+        """The ComplexF32 copy of the Green operator (made once)."""
+        if self._g32 is None:
+            if self.greens_op.dtype == np.complex64:
+                self._g32 = self.greens_op
+            else:
+                self._g32 = cast(self.greens_op, np.complex64)
+        return self._g32
+
+
+class SolveInfo:
+    """Counters of one gila_ls_solve call."""
+
+    def __init__(self, c: L.GilaSolveInfoC, res):
+        self.iters = c.iters
+        self.outer = c.outer
+        self.matvecs_f64 = c.matvecs_f64
+        self.matvecs_f32 = c.matvecs_f32
+        self.rel_res = c.rel_res
+        self.converged = c.converged
+        self.breakdowns = c.breakdowns
+        self.rhs_res = list(res)
+
+    def __repr__(self):
+        return (f"SolveInfo(iters={self.iters}, outer={self.outer}, matvecs_f64={self.matvecs_f64}, "
+                f"matvecs_f32={self.matvecs_f32}, rel_res={self.rel_res:.3e}, converged={self.converged})")
+
+
+def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, ell: int = 2,
+          inner_tol: float = 1e-4, max_matvecs: int = 4000, max_outer: int = 20, x0=None,
+          graph: bool = True, check: bool = True):
+    """Solve ls * t = i (t = (1 - chi G)^-1 i, examples/scattering_film.jl:58-61)
+    with BiCGStab(ell) on the GPU, for one field or a stack of nrhs fields.
+
+    numpy input: (Nx, Ny, Nz, 3) or (Nx, Ny, Nz, 3, nrhs); torch input:
+    (3, Nz, Ny, Nx) or (nrhs, 3, Nz, Ny, Nx); complex128 either way.  mixed
+    runs the Krylov iterations on the ComplexF32 operator inside FP64
+    iterative refinement.  Returns (t, SolveInfo); raises GilaError when a
+    right-hand side misses tol and `check` is set."""
+    G = ls.greens_op
+    if G.dtype != np.complex128:
+        raise AssertionError("the solve needs the ComplexF64 Green operator (its residual is FP64)")
+    cel = G.glaSze(1)[:3]
+    nvox = 3 * math.prod(cel)
+    if _is_torch(i):
+        import torch
+        if i.dtype != torch.complex128:
+            raise AssertionError("right-hand sides must be complex128")
+        b = i.contiguous()
+        numel = b.numel()
+        x = torch.empty_like(b)
+        bp, xp = b.data_ptr(), x.data_ptr()
+        keep = (b, x)
+    else:
+        a = np.asarray(i)
+        if a.dtype != np.complex128:
+            raise AssertionError("right-hand sides must be complex128")
+        b = np.asfortranarray(a)
+        numel = b.size
+        x = np.zeros_like(b, order="F")
+        bp, xp = b.ctypes.data, x.ctypes.data
+        keep = (b, x)
+    if numel % nvox:
+        raise DimensionMismatch(f"right-hand sides must hold whole fields of {nvox} elements")
+    nrhs = numel // nvox
+    if x0 is not None:
+        if _is_torch(x):
+            x.copy_(x0.reshape(x.shape))
+        else:
+            x[...] = np.reshape(np.asarray(x0), x.shape, order="F")
+    chi = np.asfortranarray(ls.medium.astype(np.complex128))
+    o = L.GilaSolveC(tol=tol, ell=ell, mixed=1 if mixed else 0, max_matvecs=max_matvecs, max_outer=max_outer,
+                     inner_tol=inner_tol, x0=0 if x0 is None else 1, no_graph=0 if graph else 1)
+    inf = L.GilaSolveInfoC()
+    res = (ct.c_double * nrhs)()
+    g32 = ls.g32().mem._h if mixed else None
+    st = L.lib().gila_ls_solve(G.mem._h, g32, ct.c_void_p(chi.ctypes.data), ct.c_void_p(bp), ct.c_void_p(xp),
+                               nrhs, ct.byref(o), ct.byref(inf), res, None)
+    del keep
+    info = SolveInfo(inf, res)
+    if st == L.GILA_ERR_NOTCONV and not check:
+        return x, info
+    _check(st)
+    return x, info

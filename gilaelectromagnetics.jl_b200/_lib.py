@@ -45,14 +45,16 @@ class GilaKoptC(ct.Structure):
 
 class GilaSolveC(ct.Structure):
     """gila_solve_opts (include/gila_b200.h)."""
-    _fields_ = [("tol", ct.c_double), ("max_iter", ct.c_int32), ("inner_tol", ct.c_double),
-                ("inner_max_iter", ct.c_int32), ("mixed", ct.c_int32), ("method", ct.c_int32),
-                ("restart", ct.c_int32), ("max_outer", ct.c_int32)]
+    _fields_ = [("tol", ct.c_double), ("ell", ct.c_int32), ("mixed", ct.c_int32),
+                ("max_matvecs", ct.c_int32), ("max_outer", ct.c_int32), ("inner_tol", ct.c_double),
+                ("x0", ct.c_int32), ("no_graph", ct.c_int32)]
 
 
 class GilaSolveInfoC(ct.Structure):
+    """gila_solve_info (include/gila_b200.h)."""
     _fields_ = [("iters", ct.c_int32), ("outer", ct.c_int32), ("matvecs_f64", ct.c_int32),
-                ("matvecs_f32", ct.c_int32), ("rel_res", ct.c_double), ("converged", ct.c_int32)]
+                ("matvecs_f32", ct.c_int32), ("rel_res", ct.c_double), ("converged", ct.c_int32),
+                ("breakdowns", ct.c_int32)]
 
 
 _lib = None
@@ -85,6 +87,10 @@ _SIGS = [
     ("gila_opr_device_bytes", ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int64)]),
     ("gila_opr_time_passes", ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_double * 4]),
     ("gila_opr_launches_per_apply", ct.c_int, [ct.c_void_p, ct.c_int64, ct.POINTER(ct.c_int64)]),
+    ("gila_opr_cast", ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]),
+    ("gila_ls_solve", ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,
+                                 ct.POINTER(GilaSolveC), ct.POINTER(GilaSolveInfoC), ct.POINTER(ct.c_double),
+                                 ct.c_void_p]),
     ("gila_opr_apply_noalloc", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p,
                                           ct.c_int64, ct.c_void_p]),
 ]

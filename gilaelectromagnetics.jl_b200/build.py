@@ -18,7 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgila_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["gila.cu", "matvec.cu", "noalloc.cu", "kerbuild.cu"]
+SOURCES = ["gila.cu", "matvec.cu", "noalloc.cu", "kerbuild.cu", "solver.cu"]
 HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "internal.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -259,7 +259,7 @@ static std::vector<int> axis_map(int P, int tru, int tcel) {
   return m;
 }
 
-static gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* src_abi, const gila_kopt* opt,
+gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* src_abi, const gila_kopt* opt,
                              gila_dtype dtype, std::shared_ptr<Core>& core) {
   if (!ctx || !trg_abi) return fail(GILA_ERR_ARG, "null context or target volume");
   if (dtype != GILA_C64 && dtype != GILA_C128) return fail(GILA_ERR_TYPE, "setTyp must be ComplexF32 or ComplexF64");
@@ -342,7 +342,7 @@ static gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_
   return GILA_OK;
 }
 
-static bool is_device_ptr(const void* p) {
+bool is_device_ptr(const void* p) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
@@ -401,20 +401,6 @@ static gila_status load_fur(Core& c, const void* const fur[8], gila_dtype fdt, s
   return GILA_OK;
 }
 
-template <typename C>
-static DevOp<C> devop(const Core& c) {
-  DevOp<C> d;
-  d.ker = static_cast<const C*>(c.ker);
-  for (int k = 0; k < 3; ++k) {
-    d.map[k] = c.maps[k];
-    d.tw[k] = static_cast<const C*>(c.tw[k]);
-    d.plan[k] = c.plan[k];
-    d.plan_d[k] = c.plan_d + k;
-  }
-  d.scale = 1.0 / ((double)c.geom.P[0] * c.geom.P[1] * c.geom.P[2]);
-  return d;
-}
-
 // Launch shapes: the largest tiles whose thread count stays <= 512 with 8
 // staged values per thread and whose shared memory stays within budget.
 Launch default_launch(const Core& c) {
@@ -447,7 +433,7 @@ Launch default_launch(const Core& c) {
   return L;
 }
 
-static gila_status ensure_work(Core& c, int64_t nrhs) {
+gila_status ensure_work(Core& c, int64_t nrhs) {
   if (nrhs <= c.cap_rhs) return GILA_OK;
   c.geom.max_rhs = (int)nrhs;
   const Work w = work_sizes(c.geom);
@@ -462,8 +448,8 @@ static gila_status ensure_work(Core& c, int64_t nrhs) {
   return GILA_OK;
 }
 
-static int64_t in_elems(const Core& c) { return 3LL * c.geom.sc[0] * c.geom.sc[1] * c.geom.sc[2]; }
-static int64_t out_elems(const Core& c) {
+int64_t in_elems(const Core& c) { return 3LL * c.geom.sc[0] * c.geom.sc[1] * c.geom.sc[2]; }
+int64_t out_elems(const Core& c) {
   return 3LL * c.geom.out_full[0] * c.geom.out_full[1] * c.geom.out_full[2];
 }
 

@@ -92,6 +92,26 @@ size_t csize(gila_dtype t);
 Launch default_launch(const Core& c);
 // GPU FP64 Fourier-kernel build into c.ker (kerbuild.cu)
 gila_status build_kernel(Core& c);
+gila_status ensure_work(Core& c, int64_t nrhs);
+int64_t in_elems(const Core& c);
+int64_t out_elems(const Core& c);
+bool is_device_ptr(const void* p);
+gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* src_abi, const gila_kopt* opt,
+                      gila_dtype dtype, std::shared_ptr<Core>& core);
+
+template <typename C>
+inline DevOp<C> devop(const Core& c) {
+  DevOp<C> d;
+  d.ker = static_cast<const C*>(c.ker);
+  for (int k = 0; k < 3; ++k) {
+    d.map[k] = c.maps[k];
+    d.tw[k] = static_cast<const C*>(c.tw[k]);
+    d.plan[k] = c.plan[k];
+    d.plan_d[k] = c.plan_d + k;
+  }
+  d.scale = 1.0 / ((double)c.geom.P[0] * c.geom.P[1] * c.geom.P[2]);
+  return d;
+}
 gila_status plan_axis(int P, AxisPlan* pl);
 gila_status twiddle_table(Ctx* ctx, int P, gila_dtype dt, const void** out);
 

@@ -162,6 +162,49 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 /* Number of kernels one apply of nrhs vectors launches. */
 gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n);
 
+/* ---- the scattering solve (examples/GilaOperators.jl:57-96) ------------ */
+/* A copy of the operator in another precision (kernel cast on the device),
+ * sharing nothing with the original.  Used to pair a ComplexF64 operator with
+ * the ComplexF32 one of the mixed-precision solve. */
+gila_status gila_opr_cast(gila_opr* opr, gila_dtype dtype, gila_opr** out);
+
+typedef struct {
+  double tol;           /* target FP64 relative residual ||b - A x|| / ||b||; <= 0 -> 1e-6 */
+  int32_t ell;          /* BiCGStab(l) degree 1..4; 0 -> 2 (IterativeSolvers.bicgstabl's default) */
+  int32_t mixed;        /* 0: FP64 Krylov solve; 1: ComplexF32 Krylov inner solves inside an
+                           FP64 iterative-refinement loop (FP64 residuals from the FP64 matvec) */
+  int32_t max_matvecs;  /* cap on Krylov operator applications, all inner solves; 0 -> 4000 */
+  int32_t max_outer;    /* cap on refinement steps; 0 -> 20 */
+  double inner_tol;     /* mixed: residual reduction asked of each inner solve; <= 0 -> 1e-4 */
+  int32_t x0;           /* 1: x holds an initial guess on entry; 0: start from zero (as
+                           IterativeSolvers.bicgstabl(A, b) does) */
+  int32_t no_graph;     /* 1: launch every Krylov iteration's kernels directly instead of
+                           replaying one captured CUDA graph per iteration */
+} gila_solve_opts;
+
+typedef struct {
+  int32_t iters;        /* BiCGStab(l) iterations of the batch, all inner solves (2l matvecs each) */
+  int32_t outer;        /* refinement steps (true-residual evaluations) */
+  int32_t matvecs_f64;  /* batched FP64 operator applications */
+  int32_t matvecs_f32;  /* batched ComplexF32 operator applications */
+  double rel_res;       /* max over right-hand sides of the final FP64 relative residual */
+  int32_t converged;    /* right-hand sides that reached tol */
+  int32_t breakdowns;   /* right-hand sides whose Krylov recurrence broke down at least once */
+} gila_solve_info;
+
+/* Solve (I - chi G) x = b for nrhs right-hand sides at once: the
+ * LippmannSchwinger operator of examples/GilaOperators.jl:89-96 (chi per
+ * cell, broadcast over the 3 components) and its `solve`
+ * (examples/scattering_film.jl:58-61, IterativeSolvers.bicgstabl) with
+ * BiCGStab(l).  g64 is a ComplexF64 self operator; g32 a ComplexF32 operator
+ * of the same volume (gila_opr_cast), required when opts->mixed.  chi:
+ * (Nx,Ny,Nz) complex128; b, x: (Nx,Ny,Nz,3,nrhs) complex128, host or device
+ * pointers.  opts may be NULL (defaults); info and rhs_res (nrhs final FP64
+ * relative residuals) may be NULL.  Returns GILA_ERR_NOTCONV, with x holding
+ * the last iterate, when a right-hand side missed the tolerance. */
+gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const void* b, void* x, int64_t nrhs,
+                          const gila_solve_opts* opts, gila_solve_info* info, double* rhs_res, void* stream);
+
 /* A matvec that allocates no device memory.  This entry point has no
  * counterpart in the reference.  It computes out = G * in for one vector,
  * like gila_opr_apply, for callers that cannot let the library call

@@ -1,0 +1,212 @@
+"""GPU scattering solve (gila_ls_solve) against the solve oracle.
+
+The operator is the LippmannSchwinger form of examples/GilaOperators.jl:89-95,
+A x = x - chi .* (G x), with G built on the GPU and exported (egoFur) so that
+the oracle applies exactly the same kernel on the CPU in FP64.  The plain
+solve runs the same BiCGStab(l) recurrence as oracle/solve.py from the same
+shadow residual, so iteration counts agree and iterates agree to rounding;
+every solved field is also checked through the oracle's own FP64 residual
+|b - A x| / |b| <= tol (tol = 1e-6), independent of the GPU's bookkeeping.
+"""
+from __future__ import annotations
+
+import ctypes as ct
+
+import numpy as np
+import pytest
+
+from conftest import load_pkg, rel_l2
+from oracle.gla_mem import Vol, mix_for
+from oracle.matvec import OprMem
+from oracle.solve import ls_apply, refine_solve
+from oracle.synth import seeded_current
+
+pytestmark = pytest.mark.gpu
+
+CEL = (12, 10, 8)
+SCL = ("1/32", "1/32", "1/32")
+TOL = 1e-6
+
+
+def _flat(a):
+    return np.reshape(np.asarray(a), -1, order="F")
+
+
+def _plane_wave(cel, theta_deg=80.5):
+    """s-polarised plane wave E = y exp(i 2 pi k.r), k = (sin t, 0, -cos t)
+    (examples/scattering_film.jl:79-92), cells of 1/32 wavelength."""
+    t = np.deg2rad(theta_deg)
+    k = np.array([np.sin(t), 0.0, -np.cos(t)])
+    h = 1.0 / 32
+    x, y, z = np.meshgrid(*[np.arange(n) * h for n in cel], indexing="ij")
+    ph = np.exp(2j * np.pi * (k[0] * x + k[1] * y + k[2] * z))
+    e = np.zeros((*cel, 3), dtype=np.complex128, order="F")
+    e[..., 1] = ph
+    return e
+
+
+@pytest.fixture(scope="module")
+def sys_():
+    gila = load_pkg()
+    opt = gila.GlaKerOpt(1.0 + 0j, 16, False, True, (), ())
+    G = gila.GlaOpr(gila.GlaOprMem(opt, gila.GlaVol(CEL, SCL)))
+    trg, _, mix, _ = mix_for(Vol.make(CEL, SCL, (0, 0, 0)), None)
+    mem = OprMem(mix, G.mem.egoFur)
+    chi = np.zeros(CEL, dtype=np.complex128, order="F")
+    chi[:, :, 2:6] = 3.0 + 0.1j
+    ls = gila.LippmannSchwinger(G, chi)
+    A = lambda v: ls_apply(mem, chi, v)  # noqa: E731
+    return gila, G, ls, mem, chi, A
+
+
+def _res(A, x, b):
+    x, b = _flat(x), _flat(b)
+    return np.linalg.norm(b - A(x)) / np.linalg.norm(b)
+
+
+def test_ls_operator_matches_oracle(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    x = seeded_current(CEL, 30)
+    assert rel_l2(_flat(ls * x), A(_flat(x))) < 1e-12
+
+
+def test_plain_solve_follows_oracle_bicgstabl(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 31)
+    x, info = gila.solve(ls, b, tol=TOL)
+    xo, io = refine_solve(A, _flat(b), tol=TOL)
+    assert info.converged == 1 and info.outer == io["outer"] == 1
+    assert info.iters == io["iters"]
+    assert info.matvecs_f32 == 0
+    assert rel_l2(_flat(x), xo) < 1e-9
+    r = _res(A, x, b)
+    assert r <= TOL and abs(r - info.rel_res) <= 1e-3 * r
+
+
+def test_mixed_solve_reaches_fp64_residual(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    b = _plane_wave(CEL)
+    x, info = gila.solve(ls, b, tol=TOL, mixed=True)
+    assert info.converged == 1 and info.matvecs_f32 > 0 and info.outer >= 2
+    assert _res(A, x, b) <= TOL
+    x_ref, _ = refine_solve(A, _flat(b), tol=1e-12)
+    xp, _ = gila.solve(ls, b, tol=TOL)
+    # both solves stop at residual 1e-6; the fields agree to that level
+    assert rel_l2(_flat(x), x_ref) < 1e-4
+    assert rel_l2(_flat(xp), x_ref) < 1e-4
+
+
+@pytest.mark.parametrize("mixed", [False, True])
+def test_batch_equals_alone(sys_, mixed):
+    """Each right-hand side of a batch gets the result it gets alone."""
+    gila, G, ls, mem, chi, A = sys_
+    bs = [seeded_current(CEL, 40), _plane_wave(CEL, 30.0), 0.1 * seeded_current(CEL, 41)]
+    B = np.stack(bs, axis=-1)
+    X, info = gila.solve(ls, np.asfortranarray(B), tol=TOL, mixed=mixed)
+    assert info.converged == 3
+    for k, b in enumerate(bs):
+        xk, _ = gila.solve(ls, b, tol=TOL, mixed=mixed)
+        assert rel_l2(X[..., k], xk) <= 1e-12
+        assert _res(A, X[..., k], b) <= TOL
+
+
+def test_graph_and_direct_launches_agree(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 42)
+    x1, i1 = gila.solve(ls, b, tol=TOL, mixed=True, graph=True)
+    x2, i2 = gila.solve(ls, b, tol=TOL, mixed=True, graph=False)
+    assert i1.iters == i2.iters
+    assert np.array_equal(x1, x2)
+
+
+def test_vacuum_medium_is_identity(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    ls0 = gila.LippmannSchwinger(G, np.zeros(CEL, dtype=np.complex128))
+    b = seeded_current(CEL, 43)
+    x, info = gila.solve(ls0, b, tol=TOL)
+    assert rel_l2(x, b) < 1e-14 and info.converged == 1
+
+
+def test_zero_rhs_in_batch(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 44)
+    B = np.stack([b, np.zeros_like(b)], axis=-1)
+    X, info = gila.solve(ls, np.asfortranarray(B), tol=TOL)
+    assert info.converged == 2
+    assert np.all(X[..., 1] == 0)
+    assert _res(A, X[..., 0], b) <= TOL
+
+
+def test_initial_guess(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 45)
+    x, _ = gila.solve(ls, b, tol=1e-9)
+    x2, info = gila.solve(ls, b, tol=1e-6, x0=x)
+    assert info.iters == 0 and info.converged == 1
+    assert np.array_equal(x, x2)
+
+
+@pytest.mark.parametrize("ell", [1, 4])
+def test_other_degrees(sys_, ell):
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 46)
+    x, info = gila.solve(ls, b, tol=TOL, ell=ell)
+    xo, io = refine_solve(A, _flat(b), tol=TOL, ell=ell)
+    assert info.iters == io["iters"]
+    assert _res(A, x, b) <= TOL
+
+
+def test_device_tensors(sys_):
+    import torch
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 47)
+    bt = torch.from_numpy(np.ascontiguousarray(_flat(b))).reshape(3, CEL[2], CEL[1], CEL[0]).cuda()
+    xt, info = gila.solve(ls, bt, tol=TOL, mixed=True)
+    assert xt.is_cuda and info.converged == 1
+    xn, _ = gila.solve(ls, b, tol=TOL, mixed=True)
+    assert np.array_equal(xt.cpu().numpy().reshape(-1), _flat(xn))
+
+
+def test_not_converged_and_errors(sys_):
+    gila, G, ls, mem, chi, A = sys_
+    L = gila._lib
+    b = seeded_current(CEL, 48)
+    x, info = gila.solve(ls, b, tol=TOL, max_matvecs=4, check=False)
+    assert info.converged == 0 and info.iters == 1 and info.rel_res > TOL
+    with pytest.raises(gila.GilaError):
+        gila.solve(ls, b, tol=TOL, max_matvecs=4)
+    lib = L.lib()
+    chi_c = np.asfortranarray(chi)
+    xb = np.zeros_like(b)
+    o = L.GilaSolveC(tol=TOL, ell=2, mixed=1)
+    st = lib.gila_ls_solve(G.mem._h, None, ct.c_void_p(chi_c.ctypes.data), ct.c_void_p(b.ctypes.data),
+                           ct.c_void_p(xb.ctypes.data), 1, ct.byref(o), None, None, None)
+    assert st == L.GILA_ERR_ARG
+    o = L.GilaSolveC(tol=TOL, ell=5)
+    st = lib.gila_ls_solve(G.mem._h, None, ct.c_void_p(chi_c.ctypes.data), ct.c_void_p(b.ctypes.data),
+                           ct.c_void_p(xb.ctypes.data), 1, ct.byref(o), None, None, None)
+    assert st == L.GILA_ERR_ARG
+    g32 = ls.g32()
+    st = lib.gila_ls_solve(g32.mem._h, None, ct.c_void_p(chi_c.ctypes.data), ct.c_void_p(b.ctypes.data),
+                           ct.c_void_p(xb.ctypes.data), 1, None, None, None, None)
+    assert st == L.GILA_ERR_TYPE
+    opt = gila.GlaKerOpt(1.0 + 0j, 8, False, True, (), ())
+    ext = gila.GlaOpr(gila.GlaOprMem(opt, gila.GlaVol((4, 4, 2), SCL, ("9/32", 0, 0)), gila.GlaVol((4, 4, 4), SCL)))
+    c2 = np.zeros((4, 4, 4), dtype=np.complex128)
+    b2 = np.zeros((4, 4, 4, 3), dtype=np.complex128, order="F")
+    st = lib.gila_ls_solve(ext.mem._h, None, ct.c_void_p(c2.ctypes.data), ct.c_void_p(b2.ctypes.data),
+                           ct.c_void_p(b2.ctypes.data), 1, None, None, None, None)
+    assert st == L.GILA_ERR_SIZE
+
+
+def test_cast_operator_matvec(sys_):
+    """gila_opr_cast: the ComplexF32 copy applies the same kernel rounded."""
+    gila, G, ls, mem, chi, A = sys_
+    g32 = ls.g32()
+    assert g32.dtype == np.complex64
+    x = seeded_current(CEL, 49)
+    y64 = G * x
+    y32 = g32 * x.astype(np.complex64)
+    assert rel_l2(y32, y64) < 1e-5
+    back = gila.cast(g32, np.complex128)
+    assert rel_l2(back * x, y64) < 1e-6
