@@ -635,16 +635,19 @@ class SolveInfo:
 
 
 def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, ell: int = 2,
-          inner_tol: float = 1e-4, max_matvecs: int = 4000, max_outer: int = 20, x0=None,
-          graph: bool = True, check: bool = True):
+          delta: float = 0.1, max_matvecs: int = 4000, max_restarts: int = 20, x0=None,
+          graph: bool = True, check: bool = True, stream=None):
     """Solve ls * t = i (t = (1 - chi G)^-1 i, examples/scattering_film.jl:58-61)
     with BiCGStab(ell) on the GPU, for one field or a stack of nrhs fields.
 
     numpy input: (Nx, Ny, Nz, 3) or (Nx, Ny, Nz, 3, nrhs); torch input:
     (3, Nz, Ny, Nx) or (nrhs, 3, Nz, Ny, Nx); complex128 either way.  mixed
-    runs the Krylov iterations on the ComplexF32 operator inside FP64
-    iterative refinement.  Returns (t, SolveInfo); raises GilaError when a
-    right-hand side misses tol and `check` is set."""
+    runs the Krylov process on the ComplexF32 operator with FP64 reliable
+    updates (FP64 solution; the recursive residual replaced by the FP64
+    b - A x whenever it fell by `delta`).  Returns (t, SolveInfo); raises
+    GilaError when a right-hand side misses tol and `check` is set.  With a
+    CUDA stream handle the solve is ordered after the work queued on it and
+    the stream waits for the solve."""
     G = ls.greens_op
     if G.dtype != np.complex128:
         raise AssertionError("the solve needs the ComplexF64 Green operator (its residual is FP64)")
@@ -677,13 +680,13 @@ def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, e
         else:
             x[...] = np.reshape(np.asarray(x0), x.shape, order="F")
     chi = np.asfortranarray(ls.medium.astype(np.complex128))
-    o = L.GilaSolveC(tol=tol, ell=ell, mixed=1 if mixed else 0, max_matvecs=max_matvecs, max_outer=max_outer,
-                     inner_tol=inner_tol, x0=0 if x0 is None else 1, no_graph=0 if graph else 1)
+    o = L.GilaSolveC(tol=tol, ell=ell, mixed=1 if mixed else 0, max_matvecs=max_matvecs,
+                     max_restarts=max_restarts, delta=delta, x0=0 if x0 is None else 1, no_graph=0 if graph else 1)
     inf = L.GilaSolveInfoC()
     res = (ct.c_double * nrhs)()
     g32 = ls.g32().mem._h if mixed else None
     st = L.lib().gila_ls_solve(G.mem._h, g32, ct.c_void_p(chi.ctypes.data), ct.c_void_p(bp), ct.c_void_p(xp),
-                               nrhs, ct.byref(o), ct.byref(inf), res, None)
+                               nrhs, ct.byref(o), ct.byref(inf), res, ct.c_void_p(stream) if stream else None)
     del keep
     info = SolveInfo(inf, res)
     if st == L.GILA_ERR_NOTCONV and not check:

@@ -46,7 +46,7 @@ class GilaKoptC(ct.Structure):
 class GilaSolveC(ct.Structure):
     """gila_solve_opts (include/gila_b200.h)."""
     _fields_ = [("tol", ct.c_double), ("ell", ct.c_int32), ("mixed", ct.c_int32),
-                ("max_matvecs", ct.c_int32), ("max_outer", ct.c_int32), ("inner_tol", ct.c_double),
+                ("max_matvecs", ct.c_int32), ("max_restarts", ct.c_int32), ("delta", ct.c_double),
                 ("x0", ct.c_int32), ("no_graph", ct.c_int32)]
 
 

@@ -155,9 +155,10 @@ enum FinMode : int { FIN_STORE = 0, FIN_CHECK = 1, FIN_RESID = 2, FIN_NORM = 3 }
 // fixed order.  FIN_STORE / FIN_CHECK write scalar slots (FIN_CHECK retires a
 // right-hand side whose value is zero or not finite: a breakdown);
 // FIN_RESID stores the residual norm and retires converged (nrm2 <= tol2) or
-// broken right-hand sides; FIN_NORM only stores the norm.
+// broken right-hand sides; FIN_NORM stores the squared norm in nrm_out.
 __global__ void __launch_bounds__(kT) k_fin(const double2* __restrict__ part, int K, int nb, double2* sc, int slot,
-                                            Stat* st, const double* __restrict__ tol2, int mode) {
+                                            Stat* st, const double* __restrict__ tol2, int mode,
+                                            double* __restrict__ nrm_out = nullptr) {
   const int r = blockIdx.x;
   if (mode == FIN_RESID && !st[r].act) return;
   __shared__ double2 sh[kT / 32];
@@ -182,9 +183,11 @@ __global__ void __launch_bounds__(kT) k_fin(const double2* __restrict__ part, in
           st[r].act = 0;
           st[r].broke = 1;
         }
+      } else if (mode == FIN_NORM) {
+        nrm_out[r] = t.x;
       } else {
         st[r].nrm2 = t.x;
-        if (mode == FIN_RESID) {
+        {
           if (st[r].broke || !isfinite(t.x)) {
             st[r].act = 0;
             st[r].broke = 1;
@@ -199,9 +202,10 @@ __global__ void __launch_bounds__(kT) k_fin(const double2* __restrict__ part, in
 }
 
 // ---------------------------------------------------------- scalar steps
-__global__ void k_scal_init(double2* sc, int nrhs) {
+// sigma = omega = 1 for the right-hand sides whose Krylov process (re)starts
+__global__ void k_scal_init(double2* sc, const int* __restrict__ mask, int nrhs) {
   const int r = blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= nrhs) return;
+  if (r >= nrhs || !mask[r]) return;
   sc[(int64_t)r * kSlots + S_SIG] = make_double2(1.0, 0.0);
   sc[(int64_t)r * kSlots + S_OMG] = make_double2(1.0, 0.0);
 }
@@ -365,11 +369,13 @@ __global__ void __launch_bounds__(kT) k_ls_combine(const C* __restrict__ in, C* 
 }
 
 // ------------------------------------------------- refinement (FP64) steps
-// r = b - (x - chi .* t) with t = G x held in r on entry; partial |r|^2.
+// r = b - (x - chi .* t) with t = G x held in r on entry; partial |r|^2
+// (masked right-hand sides only when mask is set).
 __global__ void __launch_bounds__(kT) k_resid(const double2* __restrict__ b, const double2* __restrict__ x,
                                               double2* __restrict__ r, const double2* __restrict__ chi, int64_t V,
-                                              double2* __restrict__ part) {
+                                              const int* __restrict__ mask, double2* __restrict__ part) {
   const int q = blockIdx.y, nb = gridDim.x;
+  if (mask && !mask[q]) return;
   const int64_t off = 3 * V * q;
   double2 acc[1] = {make_double2(0.0, 0.0)};
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < V; i += (int64_t)nb * kT) {
@@ -385,39 +391,57 @@ __global__ void __launch_bounds__(kT) k_resid(const double2* __restrict__ b, con
   block_sum_store<1>(acc, 1, part + (int64_t)q * nb + blockIdx.x, nb);
 }
 
-// Start of an inner solve on the correction equation A d = r / |r|:
-// r_0 = r64 * inv (rounded to C), x = 0, u_0 = 0; partial |r_0|^2.
+// (Re)start of the Krylov process on the scaled correction equation
+// A d = r / s for the masked right-hand sides: r_0 = r64 * inv (inv = 1/s,
+// rounded to C), d = 0, u_0 = 0.
 template <typename C>
 __global__ void __launch_bounds__(kT) k_inner_start(const double2* __restrict__ r64, KVec<C> v,
-                                                    const double* __restrict__ inv, int64_t n,
-                                                    double2* __restrict__ part) {
-  const int r = blockIdx.y, nb = gridDim.x;
+                                                    const double* __restrict__ inv, const int* __restrict__ mask,
+                                                    int64_t n) {
+  const int r = blockIdx.y;
+  if (!mask[r]) return;
   const double s = inv[r];
   const int64_t off = (int64_t)r * n;
   const C zero = from_d<C>(make_double2(0.0, 0.0));
-  double2 acc[1] = {make_double2(0.0, 0.0)};
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT) {
+  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
     const double2 a = r64[off + i];
-    const C c = from_d<C>(make_double2(a.x * s, a.y * s));
-    v.r[0][off + i] = c;
+    v.r[0][off + i] = from_d<C>(make_double2(a.x * s, a.y * s));
     v.u[0][off + i] = zero;
     v.x[off + i] = zero;
-    acc[0].x += cabs2(to_d(c));
   }
-  block_sum_store<1>(acc, 1, part + (int64_t)r * nb + blockIdx.x, nb);
 }
 
-// x64 += scale * d (scale 0: right-hand side not refined this step)
+// Reliable update, first half: x64 += s * d and d = 0 for the masked
+// right-hand sides (the correction leaves the low-precision iterate).
 template <typename C>
-__global__ void __launch_bounds__(kT) k_accum(double2* __restrict__ x, const C* __restrict__ d,
-                                              const double* __restrict__ scale, int64_t n) {
+__global__ void __launch_bounds__(kT) k_accum(double2* __restrict__ x, C* __restrict__ d,
+                                              const double* __restrict__ scale, const int* __restrict__ mask,
+                                              int64_t n) {
   const int r = blockIdx.y;
+  if (!mask[r]) return;
   const double s = scale[r];
-  if (s == 0.0) return;
   const int64_t off = (int64_t)r * n;
+  const C zero = from_d<C>(make_double2(0.0, 0.0));
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
     const double2 a = to_d(d[off + i]);
     x[off + i] = make_double2(x[off + i].x + s * a.x, x[off + i].y + s * a.y);
+    d[off + i] = zero;
+  }
+}
+
+// Reliable update, second half: the recursive residual of the masked
+// right-hand sides is replaced by the FP64 one, r_0 = (b - A64 x) * inv.
+template <typename C>
+__global__ void __launch_bounds__(kT) k_replace(const double2* __restrict__ r64, C* __restrict__ r0,
+                                                const double* __restrict__ inv, const int* __restrict__ mask,
+                                                int64_t n) {
+  const int r = blockIdx.y;
+  if (!mask[r]) return;
+  const double s = inv[r];
+  const int64_t off = (int64_t)r * n;
+  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
+    const double2 a = r64[off + i];
+    r0[off + i] = from_d<C>(make_double2(a.x * s, a.y * s));
   }
 }
 
@@ -469,8 +493,8 @@ struct DevArena {  // frees what it allocated when the solve returns
 };
 
 struct Opts {
-  double tol, inner_tol;
-  int ell, mixed, max_mv, max_outer, x0, graph;
+  double tol, delta;
+  int ell, mixed, max_mv, max_restarts, x0, graph;
 };
 
 // blocks per right-hand side of the vector kernels: a function of n only, so
@@ -496,10 +520,14 @@ cudaError_t ls_apply(Core& c, const C* chi, const C* in, C* out, int nrhs, const
   return cudaGetLastError();
 }
 
+// One batched solve.  Per right-hand side r the host keeps |b|, the FP64
+// residual norm, the scale s of the current Krylov process and the largest
+// recursive residual since the last reliable update; the device keeps the
+// Krylov vectors, the scalars and the status (act / broke / nrm2).
 template <typename CI>
 struct Solver {
   Core& g64;
-  Core& gi;  // inner operator (g64 itself when plain)
+  Core& gi;  // Krylov operator (g64 itself when plain)
   const double2* chi64;
   const CI* chii;
   const double2* b;
@@ -512,7 +540,9 @@ struct Solver {
   DevArena mem;
   double2 *r64 = nullptr, *part = nullptr, *sc = nullptr;
   Stat *st_d = nullptr, *st_h = nullptr;
-  double *tol2_d = nullptr, *scale_d = nullptr, *inv_d = nullptr, *hbuf = nullptr;
+  // parameter block [tol2 | scale | inv | nrm] doubles then [mask] ints,
+  // mirrored in pinned host memory
+  char *pb_d = nullptr, *pb_h = nullptr;
   KVec<CI> kv{};
   CI* shadow = nullptr;
   cudaGraphExec_t graph = nullptr;
@@ -527,6 +557,11 @@ struct Solver {
   ~Solver() {
     if (graph) cudaGraphExecDestroy(graph);
   }
+  double* pd(int k) const { return reinterpret_cast<double*>(pb_d) + (size_t)k * nrhs; }
+  double* ph(int k) const { return reinterpret_cast<double*>(pb_h) + (size_t)k * nrhs; }
+  int* mask_d() const { return reinterpret_cast<int*>(pb_d + 4 * sizeof(double) * nrhs); }
+  int* mask_h() const { return reinterpret_cast<int*>(pb_h + 4 * sizeof(double) * nrhs); }
+  size_t pb_bytes() const { return (4 * sizeof(double) + sizeof(int)) * (size_t)nrhs; }
 
   cudaError_t setup() {
     cudaError_t e;
@@ -535,11 +570,11 @@ struct Solver {
     if ((e = mem.alloc((void**)&part, (size_t)nrhs * kGram * nb * sizeof(double2))) != cudaSuccess) return e;
     if ((e = mem.alloc((void**)&sc, (size_t)nrhs * kSlots * sizeof(double2))) != cudaSuccess) return e;
     if ((e = mem.alloc((void**)&st_d, (size_t)nrhs * sizeof(Stat))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&tol2_d, (size_t)nrhs * 3 * sizeof(double))) != cudaSuccess) return e;
-    scale_d = tol2_d + nrhs;
-    inv_d = tol2_d + 2 * nrhs;
+    if ((e = mem.alloc((void**)&pb_d, pb_bytes())) != cudaSuccess) return e;
     if ((e = mem.alloc_host((void**)&st_h, (size_t)nrhs * sizeof(Stat))) != cudaSuccess) return e;
-    if ((e = mem.alloc_host((void**)&hbuf, (size_t)nrhs * 3 * sizeof(double))) != cudaSuccess) return e;
+    if ((e = mem.alloc_host((void**)&pb_h, pb_bytes())) != cudaSuccess) return e;
+    memset(pb_h, 0, pb_bytes());
+    memset(st_h, 0, (size_t)nrhs * sizeof(Stat));
     CI* base = nullptr;
     const int nvec = 2 * o.ell + 3;
     if ((e = mem.alloc((void**)&base, (size_t)nvec * vb * sizeof(CI))) != cudaSuccess) return e;
@@ -554,71 +589,95 @@ struct Solver {
     // every Krylov vector starts finite, including those of right-hand sides
     // that never iterate (their matvecs still run inside the batch)
     if ((e = cudaMemsetAsync(base, 0, (size_t)nvec * vb * sizeof(CI), s)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(st_d, st_h, (size_t)nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+      return e;
     k_shadow<CI><<<nb, kT, 0, s>>>(shadow, n, 0x5EEDull);
     return cudaGetLastError();
   }
 
-  // squared norms of the nrhs vectors at p (written by a kernel into part) -> host
+  // squared norms of the nrhs vectors whose partials are in `part` -> host
   cudaError_t fetch_norms(std::vector<double>& out) {
-    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2_d, FIN_NORM);
+    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, pd(0), FIN_NORM, pd(3));
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    if ((e = cudaMemcpyAsync(st_h, st_d, nrhs * sizeof(Stat), cudaMemcpyDeviceToHost, s)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(ph(3), pd(3), nrhs * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
+      return e;
     if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    out.resize(nrhs);
-    for (int r = 0; r < nrhs; ++r) out[r] = st_h[r].nrm2;
+    out.assign(ph(3), ph(3) + nrhs);
     return cudaSuccess;
   }
 
-  // r64 = b - A64 x, returns |r|^2 per right-hand side
-  cudaError_t true_residual(std::vector<double>& rn2) {
-    cudaError_t e = ls_apply_raw64(x, r64);
-    if (e != cudaSuccess) return e;
-    k_resid<<<dim3(nb, nrhs), kT, 0, s>>>(b, x, r64, chi64, n / 3, part);
+  // r64 = b - A64 x for the right-hand sides set in mask_h (all when null):
+  // one batched FP64 matvec per run of consecutive masked right-hand sides.
+  // Returns |r|^2 per right-hand side (entries of unmasked ones undefined).
+  cudaError_t true_residual(std::vector<double>& rn2, const int* mh) {
+    cudaError_t e;
+    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
+    for (int r0 = 0; r0 < nrhs;) {
+      if (mh && !mh[r0]) {
+        ++r0;
+        continue;
+      }
+      int r1 = r0 + 1;
+      while (r1 < nrhs && (!mh || mh[r1])) ++r1;
+      e = launch_matvec<double2>(g64.geom, devop<double2>(g64), g64.launch, x + (size_t)r0 * n, r64 + (size_t)r0 * n,
+                                 static_cast<double2*>(g64.A), static_cast<double2*>(g64.B), r1 - r0, false, one,
+                                 zero, s);
+      if (e != cudaSuccess) return e;
+      r0 = r1;
+    }
+    k_resid<<<dim3(nb, nrhs), kT, 0, s>>>(b, x, r64, chi64, n / 3, mh ? mask_d() : nullptr, part);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     ++info.matvecs_f64;
     return fetch_norms(rn2);
   }
 
-  // r64 = G64 in (no combine; k_resid folds chi in)
-  cudaError_t ls_apply_raw64(const double2* in, double2* out) {
-    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
-    return launch_matvec<double2>(g64.geom, devop<double2>(g64), g64.launch, in, out, static_cast<double2*>(g64.A),
-                                  static_cast<double2*>(g64.B), nrhs, false, one, zero, s);
+  // Reliable update of the masked right-hand sides (mask_h set by the
+  // caller): x64 += s d, d = 0, FP64 residual, r_0 = r64 / s.
+  cudaError_t reliable_update(std::vector<double>& rn2) {
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(pb_d, pb_h, pb_bytes(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    k_accum<CI><<<dim3(nb, nrhs), kT, 0, s>>>(x, kv.x, pd(1), mask_d(), n);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = true_residual(rn2, mask_h())) != cudaSuccess) return e;
+    k_replace<CI><<<dim3(nb, nrhs), kT, 0, s>>>(r64, kv.r[0], pd(2), mask_d(), n);
+    ++info.outer;
+    return cudaGetLastError();
   }
 
-  // One BiCGStab(l) iteration for every active right-hand side, ending with
-  // the copy of the per-rhs status to the host.
+  // One BiCGStab(l) cycle for every active right-hand side, ending with the
+  // copy of the per-rhs status to the host.
   cudaError_t body() {
     cudaError_t e;
     const dim3 gv(nb, nrhs);
     const int sb = (nrhs + 127) / 128;
+    double* tol2 = pd(0);
     k_iter_start<<<sb, 128, 0, s>>>(sc, st_d, nrhs);
     for (int j = 1; j <= o.ell; ++j) {
       k_dot<CI, CI><<<gv, kT, 0, s>>>(shadow, 0, kv.r[j - 1], n, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_RHO, st_d, tol2_d, FIN_CHECK);
+      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_RHO, st_d, tol2, FIN_CHECK);
       k_bicg_u<CI><<<gv, kT, 0, s>>>(kv, j, n, sc, st_d);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if ((e = ls_apply<CI>(gi, chii, kv.u[j - 1], kv.u[j], nrhs, st_d, nb, s)) != cudaSuccess) return e;
       k_dot<CI, CI><<<gv, kT, 0, s>>>(shadow, 0, kv.u[j], n, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_SIG, st_d, tol2_d, FIN_CHECK);
+      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_SIG, st_d, tol2, FIN_CHECK);
       k_bicg_r<CI><<<gv, kT, 0, s>>>(kv, j, n, sc, st_d, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2_d, FIN_RESID);
+      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2, FIN_RESID);
       if ((e = cudaGetLastError()) != cudaSuccess) return e;
       if ((e = ls_apply<CI>(gi, chii, kv.r[j - 1], kv.r[j], nrhs, st_d, nb, s)) != cudaSuccess) return e;
     }
     k_gram<CI><<<gv, kT, 0, s>>>(kv, o.ell, n, part);
-    k_fin<<<nrhs, kT, 0, s>>>(part, kGram, nb, sc, S_GRAM, st_d, tol2_d, FIN_STORE);
+    k_fin<<<nrhs, kT, 0, s>>>(part, kGram, nb, sc, S_GRAM, st_d, tol2, FIN_STORE);
     k_mr_solve<<<sb, 128, 0, s>>>(sc, st_d, o.ell, nrhs);
     k_mr_update<CI><<<gv, kT, 0, s>>>(kv, o.ell, n, sc, st_d, part);
-    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2_d, FIN_RESID);
+    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2, FIN_RESID);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     return cudaMemcpyAsync(st_h, st_d, nrhs * sizeof(Stat), cudaMemcpyDeviceToHost, s);
   }
 
   cudaError_t iterate(bool first) {
     if (o.graph && graph_ok && !graph && !first) {
-      // the first iteration ran directly (function attributes are set); capture the next
+      // the first cycle ran directly (function attributes are set); capture the next
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
@@ -643,84 +702,123 @@ struct Solver {
     cudaError_t e;
     const size_t vb = (size_t)nrhs * n;
     std::vector<double> bn2, rn2;
-    // |b|
     k_dot<double2, double2><<<dim3(nb, nrhs), kT, 0, s>>>(b, n, b, n, part);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     if ((e = fetch_norms(bn2)) != cudaSuccess) return e;
     if (o.x0) {
-      if ((e = true_residual(rn2)) != cudaSuccess) return e;
+      if ((e = true_residual(rn2, nullptr)) != cudaSuccess) return e;
     } else {
       if ((e = cudaMemsetAsync(x, 0, vb * sizeof(double2), s)) != cudaSuccess) return e;
       if ((e = cudaMemcpyAsync(r64, b, vb * sizeof(double2), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
       rn2 = bn2;
     }
-    std::vector<double> bn(nrhs), rn(nrhs);
-    std::vector<char> stalled(nrhs, 0), broke(nrhs, 0);
+    std::vector<double> bn(nrhs), rn(nrhs), scale(nrhs, 0.0), maxr(nrhs, 0.0);
+    std::vector<char> live(nrhs, 0), restart(nrhs, 0), broke(nrhs, 0), pending(nrhs, 0);
+    std::vector<int> restarts(nrhs, 0);
     for (int r = 0; r < nrhs; ++r) {
       bn[r] = std::sqrt(bn2[r]);
       rn[r] = std::sqrt(rn2[r]);
     }
     auto done = [&](int r) { return bn[r] == 0.0 || rn[r] <= o.tol * bn[r]; };
-    int mv = 0;
+    for (int r = 0; r < nrhs; ++r) restart[r] = !done(r) && std::isfinite(rn[r]);
+    const double delta = o.mixed ? o.delta : 0.0;
     const int mv_iter = 2 * o.ell;
-    for (int outer = 0;; ++outer) {
-      int nact = 0;
+    int mv = 0;
+    int* mh = mask_h();
+    for (;;) {
+      // (re)start the Krylov processes that need it, on A d = r / |r|
+      int nstart = 0;
       for (int r = 0; r < nrhs; ++r) {
-        const bool a = !done(r) && !stalled[r] && std::isfinite(rn[r]);
-        double* sc_h = hbuf;
-        sc_h[r] = 0.0;               // tol2
-        sc_h[nrhs + r] = 0.0;        // scale
-        sc_h[2 * nrhs + r] = 0.0;    // inv
-        st_h[r].act = a ? 1 : 0;
+        mh[r] = 0;
+        if (!restart[r]) continue;
+        restart[r] = 0;
+        if (restarts[r] >= o.max_restarts) continue;
+        ++restarts[r];
+        mh[r] = 1;
+        ++nstart;
+        live[r] = 1;
+        scale[r] = rn[r];
+        maxr[r] = 1.0;
+        st_h[r].nrm2 = 1.0;
+        st_h[r].act = 1;
         st_h[r].broke = 0;
-        st_h[r].nrm2 = 0.0;
-        if (a) {
-          ++nact;
-          // the last refinement step only has to reach the overall target
-          double t = 0.9 * o.tol * bn[r] / rn[r];
-          if (o.mixed) t = std::max(t, o.inner_tol);
-          sc_h[r] = t * t;
-          sc_h[nrhs + r] = rn[r];
-          sc_h[2 * nrhs + r] = 1.0 / rn[r];
+      }
+      if (nstart) {
+        for (int r = 0; r < nrhs; ++r) {
+          const double t = live[r] ? 0.9 * o.tol * bn[r] / scale[r] : 0.0;
+          ph(0)[r] = t * t;
+          ph(1)[r] = live[r] ? scale[r] : 0.0;
+          ph(2)[r] = live[r] ? 1.0 / scale[r] : 0.0;
+        }
+        if ((e = cudaMemcpyAsync(pb_d, pb_h, pb_bytes(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+        if ((e = cudaMemcpyAsync(st_d, st_h, nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess)
+          return e;
+        k_inner_start<CI><<<dim3(nb, nrhs), kT, 0, s>>>(r64, kv, pd(2), mask_d(), n);
+        k_scal_init<<<(nrhs + 127) / 128, 128, 0, s>>>(sc, mask_d(), nrhs);
+        if ((e = cudaGetLastError()) != cudaSuccess) return e;
+      }
+      int nlive = 0;
+      for (int r = 0; r < nrhs; ++r) nlive += live[r];
+      if (nlive == 0 || mv + mv_iter > o.max_mv) break;
+      // one cycle; its status copy is read after the sync
+      if ((e = iterate(info.iters == 0)) != cudaSuccess) return e;
+      if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+      mv += mv_iter;
+      ++info.iters;
+      if (o.mixed)
+        info.matvecs_f32 += mv_iter;
+      else
+        info.matvecs_f64 += mv_iter;
+      // reliable updates: breakdown, claimed convergence, or (mixed) a
+      // recursive residual below delta times its largest value since the last
+      int nupd = 0;
+      for (int r = 0; r < nrhs; ++r) {
+        mh[r] = 0;
+        if (!live[r]) continue;
+        pending[r] = 1;
+        const Stat& q = st_h[r];
+        const double nr = std::sqrt(q.nrm2);
+        if (q.broke || !q.act || nr < delta * maxr[r]) {
+          mh[r] = 1;
+          ++nupd;
+        } else if (nr > maxr[r]) {
+          maxr[r] = nr;
         }
       }
-      if (nact == 0 || outer >= o.max_outer || mv + mv_iter > o.max_mv) break;
-      if ((e = cudaMemcpyAsync(tol2_d, hbuf, 3 * nrhs * sizeof(double), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-        return e;
-      if ((e = cudaMemcpyAsync(st_d, st_h, nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
-      k_inner_start<CI><<<dim3(nb, nrhs), kT, 0, s>>>(r64, kv, inv_d, n, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2_d, FIN_RESID);
-      k_scal_init<<<(nrhs + 127) / 128, 128, 0, s>>>(sc, nrhs);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      // inner BiCGStab(l); the status copy of each iteration is read after it
-      bool first = info.iters == 0;
-      for (;;) {
-        if (mv + mv_iter > o.max_mv) break;
-        if ((e = iterate(first)) != cudaSuccess) return e;
-        first = false;
-        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-        mv += mv_iter;
-        ++info.iters;
-        if (o.mixed)
-          info.matvecs_f32 += mv_iter;
-        else
-          info.matvecs_f64 += mv_iter;
-        int still = 0;
-        for (int r = 0; r < nrhs; ++r) still += st_h[r].act;
-        if (still == 0) break;
-      }
-      for (int r = 0; r < nrhs; ++r) broke[r] |= (char)st_h[r].broke;
-      k_accum<CI><<<dim3(nb, nrhs), kT, 0, s>>>(x, kv.x, scale_d, n);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      std::vector<double> prev = rn;
-      if ((e = true_residual(rn2)) != cudaSuccess) return e;
-      ++info.outer;
+      if (nupd == 0) continue;
+      if ((e = reliable_update(rn2)) != cudaSuccess) return e;
       for (int r = 0; r < nrhs; ++r) {
-        const bool was = hbuf[nrhs + r] != 0.0;
+        if (!mh[r]) continue;
+        pending[r] = 0;
         rn[r] = std::sqrt(rn2[r]);
-        // a refinement step that does not halve the residual will not converge
-        if (was && !done(r) && !(rn[r] < 0.5 * prev[r])) stalled[r] = 1;
+        Stat& q = st_h[r];
+        broke[r] |= (char)q.broke;
+        if (done(r)) {
+          live[r] = 0;
+          q.act = 0;
+        } else if (q.broke || !q.act || !std::isfinite(rn[r])) {
+          // breakdown, or convergence the FP64 residual does not confirm:
+          // restart from the FP64 residual
+          live[r] = 0;
+          q.act = 0;
+          restart[r] = std::isfinite(rn[r]);
+        } else {
+          maxr[r] = rn[r] / scale[r];
+          q.nrm2 = maxr[r] * maxr[r];
+        }
       }
+      if ((e = cudaMemcpyAsync(st_d, st_h, nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
+    }
+    // fold the corrections still held by the Krylov iterates into x
+    int npend = 0;
+    for (int r = 0; r < nrhs; ++r) {
+      mh[r] = pending[r];
+      npend += pending[r];
+    }
+    if (npend) {
+      if ((e = reliable_update(rn2)) != cudaSuccess) return e;
+      for (int r = 0; r < nrhs; ++r)
+        if (pending[r]) rn[r] = std::sqrt(rn2[r]);
     }
     res.resize(nrhs);
     info.converged = 0;
@@ -809,8 +907,8 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   o.ell = opts && opts->ell > 0 ? opts->ell : 2;
   o.mixed = opts ? (opts->mixed != 0) : 0;
   o.max_mv = opts && opts->max_matvecs > 0 ? opts->max_matvecs : 4000;
-  o.max_outer = opts && opts->max_outer > 0 ? opts->max_outer : 20;
-  o.inner_tol = opts && opts->inner_tol > 0 ? opts->inner_tol : 1e-4;
+  o.max_restarts = opts && opts->max_restarts > 0 ? opts->max_restarts : 20;
+  o.delta = opts && opts->delta > 0 ? opts->delta : 0.1;
   o.x0 = opts ? (opts->x0 != 0) : 0;
   o.graph = opts ? (opts->no_graph == 0) : 1;
   if (const char* ev = getenv("GILA_SOLVE_GRAPH"))

@@ -171,20 +171,23 @@ gila_status gila_opr_cast(gila_opr* opr, gila_dtype dtype, gila_opr** out);
 typedef struct {
   double tol;           /* target FP64 relative residual ||b - A x|| / ||b||; <= 0 -> 1e-6 */
   int32_t ell;          /* BiCGStab(l) degree 1..4; 0 -> 2 (IterativeSolvers.bicgstabl's default) */
-  int32_t mixed;        /* 0: FP64 Krylov solve; 1: ComplexF32 Krylov inner solves inside an
-                           FP64 iterative-refinement loop (FP64 residuals from the FP64 matvec) */
-  int32_t max_matvecs;  /* cap on Krylov operator applications, all inner solves; 0 -> 4000 */
-  int32_t max_outer;    /* cap on refinement steps; 0 -> 20 */
-  double inner_tol;     /* mixed: residual reduction asked of each inner solve; <= 0 -> 1e-4 */
+  int32_t mixed;        /* 0: FP64 Krylov process; 1: the Krylov process runs on the ComplexF32
+                           operator and FP64 reliable updates (FP64 solution, residual replaced
+                           by the FP64 b - A x) keep the result at FP64 accuracy */
+  int32_t max_matvecs;  /* cap on Krylov operator applications; 0 -> 4000 */
+  int32_t max_restarts; /* cap on Krylov (re)starts per right-hand side (breakdowns, convergence
+                           the FP64 residual does not confirm); 0 -> 20 */
+  double delta;         /* mixed: a reliable update follows a cycle whose recursive residual fell
+                           below delta times its largest value since the last update; <= 0 -> 0.1 */
   int32_t x0;           /* 1: x holds an initial guess on entry; 0: start from zero (as
                            IterativeSolvers.bicgstabl(A, b) does) */
-  int32_t no_graph;     /* 1: launch every Krylov iteration's kernels directly instead of
-                           replaying one captured CUDA graph per iteration */
+  int32_t no_graph;     /* 1: launch every Krylov cycle's kernels directly instead of replaying
+                           one captured CUDA graph per cycle */
 } gila_solve_opts;
 
 typedef struct {
-  int32_t iters;        /* BiCGStab(l) iterations of the batch, all inner solves (2l matvecs each) */
-  int32_t outer;        /* refinement steps (true-residual evaluations) */
+  int32_t iters;        /* BiCGStab(l) cycles of the batch (2l matvecs each) */
+  int32_t outer;        /* FP64 residual evaluations (reliable updates) */
   int32_t matvecs_f64;  /* batched FP64 operator applications */
   int32_t matvecs_f32;  /* batched ComplexF32 operator applications */
   double rel_res;       /* max over right-hand sides of the final FP64 relative residual */

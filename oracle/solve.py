@@ -10,9 +10,11 @@ TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
   residual norm falls to reltol * |b| or the matvec budget is used.
   IterativeSolvers is not vendored or pinned by the reference (it appears in
   the examples only); ``bicgstabl`` below restates the published method.
-* ``refine_solve`` is the FP64 iterative-refinement loop the GPU solver wraps
-  around BiCGStab(l) (no reference counterpart: the reference solves in one
-  precision); with FP64 inner solves it is the plain GPU solve step for step.
+* ``reliable_solve`` is the GPU solver's algorithm: BiCGStab(l) with
+  reliable updates (FP64 solution and FP64 residual replacement) around a
+  Krylov process on the ComplexF32 (mixed) or ComplexF64 (plain) operator
+  (no reference counterpart: the reference solves in one precision); with
+  the FP64 operator it is the plain GPU solve step for step.
 
 Vectors are flat in the reference's memory order: (Nx, Ny, Nz, 3) column-major.
 """
@@ -57,107 +59,149 @@ def ls_apply(mem: OprMem, chi: np.ndarray, x: np.ndarray) -> np.ndarray:
     return np.reshape(x4 - chi[..., None] * g, -1, order="F")
 
 
+class _Krylov:
+    """State of one BiCGStab(l) process (Sleijpen & Fokkema 1993) on the
+    operator `apply`: residuals R[0..l], search directions U[0..l], the
+    iterate x, and the scalars sigma, omega; shadow residual rs."""
+
+    def __init__(self, apply, r0: np.ndarray, ell: int, rs: np.ndarray):
+        n = r0.size
+        self.apply, self.ell, self.rs = apply, ell, rs
+        self.R = np.zeros((ell + 1, n), dtype=np.complex128)
+        self.U = np.zeros((ell + 1, n), dtype=np.complex128)
+        self.R[0] = r0
+        self.x = np.zeros(n, dtype=np.complex128)
+        self.sigma = self.omega = 1.0 + 0j
+
+    def cycle(self, tolerance: float):
+        """One l-step cycle.  Returns (nrm, state): state "ok", "conv" (the
+        residual reached `tolerance` inside the cycle, which then ends) or
+        "broke" (a zero or non-finite rho, sigma or MR system, or omega = 0
+        after the update)."""
+        R, U, rs, ell = self.R, self.U, self.rs, self.ell
+        self.sigma = -self.omega * self.sigma
+        for j in range(1, ell + 1):          # BiCG part
+            rho = np.vdot(rs, R[j - 1])
+            if rho == 0 or not np.isfinite(rho):
+                return np.linalg.norm(R[0]), "broke"
+            beta = rho / self.sigma
+            U[:j] = R[:j] - beta * U[:j]
+            U[j] = self.apply(U[j - 1])
+            self.sigma = np.vdot(rs, U[j])
+            if self.sigma == 0 or not np.isfinite(self.sigma):
+                return np.linalg.norm(R[0]), "broke"
+            alpha = rho / self.sigma
+            R[:j] -= alpha * U[1:j + 1]
+            self.x += alpha * U[0]
+            nrm = np.linalg.norm(R[0])
+            # a residual that a BiCG step already brought to tolerance ends
+            # the cycle: the next step would divide rounding noise by rounding
+            # noise (its sigma is rho - beta * rho_prev)
+            if nrm <= tolerance:
+                return nrm, "conv"
+            R[j] = self.apply(R[j - 1])
+        M = np.conj(R) @ R.T                 # minimal-residual part
+        try:
+            gamma = np.linalg.solve(M[1:, 1:], M[1:, 0])
+        except np.linalg.LinAlgError:
+            return np.linalg.norm(R[0]), "broke"
+        if not np.all(np.isfinite(gamma)):
+            return np.linalg.norm(R[0]), "broke"
+        U[0] -= gamma @ U[1:]
+        self.x += gamma @ R[:ell]
+        R[0] -= gamma @ R[1:]
+        self.omega = gamma[-1]
+        nrm = np.linalg.norm(R[0])
+        if self.omega == 0:
+            return nrm, "broke"
+        return nrm, ("conv" if nrm <= tolerance else "ok")
+
+
 def bicgstabl(apply, b: np.ndarray, ell: int = 2, reltol: float = np.sqrt(np.finfo(float).eps),
               max_mv: int | None = None, rs: np.ndarray | None = None):
-    """BiCGStab(l) from a zero initial guess.  Returns (x, info) with info
-    iters (l-step cycles), mv (operator applications) and nrm (final
-    recursively updated residual norm)."""
+    """BiCGStab(l) from a zero initial guess, stopping on the recursively
+    updated residual (IterativeSolvers.bicgstabl's criterion).  Returns
+    (x, info) with iters (l-step cycles), mv (operator applications), nrm
+    (final recursive residual norm) and broke."""
     n = b.size
     if max_mv is None:
         max_mv = n
     if rs is None:
         rs = shadow(n)
-    x = np.zeros(n, dtype=np.complex128)
-    R = np.zeros((ell + 1, n), dtype=np.complex128)
-    U = np.zeros((ell + 1, n), dtype=np.complex128)
-    R[0] = b
-    nrm = np.linalg.norm(R[0])
+    k = _Krylov(apply, b, ell, rs)
+    nrm = np.linalg.norm(b)
     tolerance = reltol * nrm
-    sigma = omega = 1.0 + 0j
     mv = it = 0
-    broke = False
-    while not (mv >= max_mv or nrm <= tolerance):
-        # a zero or non-finite rho, sigma or MR system ends the solve at the
-        # current iterate (the GPU solver retires the right-hand side there),
-        # and so does a residual that a BiCG step already brought to
-        # tolerance (the next step would divide rounding noise by rounding
-        # noise: its sigma is rho - beta * rho_prev)
-        sigma = -omega * sigma
-        for j in range(1, ell + 1):          # BiCG part
-            rho = np.vdot(rs, R[j - 1])
-            if rho == 0 or not np.isfinite(rho):
-                broke = True
-                break
-            beta = rho / sigma
-            U[:j] = R[:j] - beta * U[:j]
-            U[j] = apply(U[j - 1])
-            sigma = np.vdot(rs, U[j])
-            if sigma == 0 or not np.isfinite(sigma):
-                broke = True
-                break
-            alpha = rho / sigma
-            R[:j] -= alpha * U[1:j + 1]
-            x += alpha * U[0]
-            nrm = np.linalg.norm(R[0])
-            if nrm <= tolerance:             # converged inside the BiCG part
-                break
-            R[j] = apply(R[j - 1])
+    state = "ok"
+    while not (mv >= max_mv or nrm <= tolerance or state == "broke"):
+        nrm, state = k.cycle(tolerance)
         mv += 2 * ell
         it += 1
-        if broke or nrm <= tolerance:
-            break
-        M = np.conj(R) @ R.T                 # minimal-residual part
-        try:
-            gamma = np.linalg.solve(M[1:, 1:], M[1:, 0])
-        except np.linalg.LinAlgError:
-            broke = True
-            break
-        if not np.all(np.isfinite(gamma)):
-            broke = True
-            break
-        U[0] -= gamma @ U[1:]
-        x += gamma @ R[:ell]
-        R[0] -= gamma @ R[1:]
-        omega = gamma[-1]
-        nrm = np.linalg.norm(R[0])
-        if omega == 0:
-            broke = True
-            break
-    return x, {"iters": it, "mv": mv, "nrm": nrm, "broke": broke}
+    return k.x, {"iters": it, "mv": mv, "nrm": nrm, "broke": state == "broke"}
 
 
-def refine_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inner_apply=None,
-                 inner_tol: float = 1e-4, max_outer: int = 20, max_mv: int = 4000):
-    """FP64 iterative refinement around BiCGStab(l), the GPU solver's outer
-    loop: r = b - A x; the correction equation A d = r / |r| is solved to
-    relative residual t = 0.9 tol |b| / |r| (mixed: at least inner_tol) by
-    BiCGStab(l) on `inner_apply` (FP64 `apply64` when None); x += |r| d.
-    Returns (x, info)."""
-    mixed = inner_apply is not None
+def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inner_apply=None,
+                   delta: float = 0.1, max_mv: int = 4000, max_restarts: int = 20, rs=None):
+    """The GPU solver's algorithm: BiCGStab(l) on `inner_apply` (FP64
+    `apply64` when None) with reliable updates (residual replacement, van der
+    Vorst & Ye 2000; its mixed-precision form as in Clark et al. 2010).
+
+    The Krylov process runs on the scaled system A d = r / s (s = |r| at its
+    start).  After a cycle whose recursive residual fell below delta times
+    its largest value since the last update (mixed only; delta = 0 for the
+    plain solve), claimed convergence (0.9 tol |b| / s), or broke down: the
+    correction is folded into the FP64 solution, x += s d, d = 0, and the
+    recursive residual is replaced by the FP64 one, r = (b - A64 x) / s,
+    keeping the search directions.  A breakdown, or claimed convergence that
+    the FP64 residual does not confirm, restarts the process from r.
+    Returns (x, info): iters, updates (FP64 residuals), mv, rel_res."""
+    n = b.size
+    if rs is None:
+        rs = shadow(n)
     inner = inner_apply or apply64
+    d = delta if inner_apply is not None else 0.0
     x = np.zeros_like(b)
-    r = b.copy()
     bn = np.linalg.norm(b)
+    r = b.copy()
     rn = bn
-    info = {"iters": 0, "outer": 0, "mv": 0}
+    info = {"iters": 0, "updates": 0, "mv": 0, "restarts": 0}
+
+    def done():
+        return bn == 0 or rn <= tol * bn
+
     mv = 0
-    for outer in range(max_outer):
-        if bn == 0 or rn <= tol * bn:
-            break
+    k = None
+    while not done():
+        if k is None:
+            if info["restarts"] >= max_restarts:
+                break
+            s = rn
+            k = _Krylov(inner, r / s, ell, rs)
+            maxr = 1.0
+            info["restarts"] += 1
         if mv + 2 * ell > max_mv:
             break
-        t = 0.9 * tol * bn / rn
-        if mixed:
-            t = max(t, inner_tol)
-        d, inf = bicgstabl(inner, r / rn, ell=ell, reltol=t, max_mv=max_mv - mv)
-        mv += inf["mv"]
-        info["iters"] += inf["iters"]
-        x = x + rn * d
+        nrm, state = k.cycle(0.9 * tol * bn / s)
+        mv += 2 * ell
+        info["iters"] += 1
+        if state == "ok" and not nrm < d * maxr:
+            maxr = max(maxr, nrm)
+            continue
+        x = x + s * k.x                      # reliable update
+        k.x[:] = 0
         r = b - apply64(x)
-        prev, rn = rn, np.linalg.norm(r)
-        info["outer"] += 1
-        if not rn < 0.5 * prev and rn > tol * bn:
-            break
+        rn = np.linalg.norm(r)
+        info["updates"] += 1
+        if state == "ok":
+            k.R[0] = r / s
+            maxr = rn / s
+        else:
+            k = None                         # restart (from r) unless done
+    if k is not None and np.any(k.x):
+        x = x + s * k.x
+        r = b - apply64(x)
+        rn = np.linalg.norm(r)
+        info["updates"] += 1
     info["mv"] = mv
     info["rel_res"] = 0.0 if bn == 0 else rn / bn
     return x, info
