@@ -20,6 +20,7 @@ The names, argument meanings and error behaviour follow the reference:
   LippmannSchwinger(G, medium), ls * x, mul(y, ls, x)
                                                    examples/GilaOperators.jl:57-96
   solve(ls, i)               BiCGStab(l) solve     examples/scattering_film.jl:58-61
+  SolveServer                continuous-batching solve server (no reference counterpart)
 
 Vectors use the reference's memory layout: (Nx, Ny, Nz, 3) column-major.
 numpy arrays are passed as shape (Nx, Ny, Nz, 3) in Fortran order (or flat);
@@ -41,7 +42,7 @@ __all__ = [
     "GlaVol", "GlaKerOpt", "GlaOprMem", "GlaOpr", "egoOpr", "mul", "adjoint", "isadjoint",
     "isselfoperator", "isexternaloperator", "glaSze", "size", "eltype", "issymmetric",
     "isposdef", "ishermitian", "isdiag", "GilaError", "DimensionMismatch", "ArgumentError",
-    "Context", "default_context", "cast", "LippmannSchwinger", "solve", "SolveInfo",
+    "Context", "default_context", "cast", "LippmannSchwinger", "solve", "SolveInfo", "SolveServer",
 ]
 
 
@@ -693,3 +694,69 @@ def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, e
         return x, info
     _check(st)
     return x, info
+
+
+class SolveServer:
+    """Continuous-batching server of scattering solves (gila_server_*).
+
+    submit(cel, scl, chi, b, tol=...) queues (I - chi G) x = b for the self
+    volume of `cel` cells of scale `scl` and returns a ticket; wait(ticket)
+    returns (x, SolveInfo, latency_ms).  Requests of the same shape share a
+    batch of slots on the GPU and join it while it runs; shapes run
+    concurrently; admission is by device memory (hbm_budget bytes, 0: free
+    memory minus 4 GiB).  numpy inputs: chi (Nx,Ny,Nz), b (Nx,Ny,Nz,3),
+    complex128."""
+
+    def __init__(self, *, slots: int = 8, ell: int = 2, mixed: bool = True, hbm_budget: int = 0,
+                 intOrd: int = 32, frqPhz: complex = 1.0 + 0j, ctx: Optional[Context] = None):
+        self.ctx = ctx or default_context()
+        o = L.GilaServerOptsC(hbm_budget=int(hbm_budget), slots=int(slots), ell=int(ell), mixed=1 if mixed else 0,
+                              int_ord=int(intOrd), frq_re=complex(frqPhz).real, frq_im=complex(frqPhz).imag)
+        h = ct.c_void_p()
+        _check(L.lib().gila_server_create(self.ctx.handle, ct.byref(o), ct.byref(h)))
+        self._h = h
+        self._live = {}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            L.lib().gila_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, cel, scl, chi, b, *, tol: float = 1e-6, max_matvecs: int = 4000, delta: float = 0.1,
+               max_restarts: int = 20) -> int:
+        v = GlaVol(cel, scl).to_c()
+        chi_a = np.asfortranarray(np.asarray(chi, dtype=np.complex128))
+        b_a = np.asfortranarray(np.asarray(b, dtype=np.complex128))
+        if chi_a.shape != tuple(cel) or b_a.shape != (*cel, 3):
+            raise DimensionMismatch("medium (Nx,Ny,Nz) and field (Nx,Ny,Nz,3) must match the volume")
+        x = np.zeros_like(b_a, order="F")
+        o = L.GilaSolveC(tol=tol, max_matvecs=max_matvecs, delta=delta, max_restarts=max_restarts)
+        t = ct.c_uint64()
+        _check(L.lib().gila_server_submit(self._h, ct.byref(v), ct.c_void_p(chi_a.ctypes.data),
+                                          ct.c_void_p(b_a.ctypes.data), ct.c_void_p(x.ctypes.data), ct.byref(o),
+                                          ct.byref(t)))
+        self._live[t.value] = (chi_a, b_a, x)
+        return t.value
+
+    def wait(self, ticket: int, timeout_ms: int = -1, check: bool = True):
+        inf = L.GilaSolveInfoC()
+        lat = ct.c_double()
+        st = L.lib().gila_server_wait(self._h, ct.c_uint64(ticket), int(timeout_ms), ct.byref(inf), ct.byref(lat))
+        if st == L.GILA_ERR_TIMEOUT:
+            raise TimeoutError(L.last_error())
+        bufs = self._live.pop(ticket, None)
+        info = SolveInfo(inf, [inf.rel_res])
+        if not (st == L.GILA_ERR_NOTCONV and not check):
+            _check(st)
+        return (bufs[2] if bufs else None), info, lat.value
+
+    def stats(self) -> dict:
+        s = L.GilaServerStatsC()
+        _check(L.lib().gila_server_stats_get(self._h, ct.byref(s)))
+        return {k: getattr(s, k) for k, _ in s._fields_}

@@ -57,6 +57,19 @@ class GilaSolveInfoC(ct.Structure):
                 ("breakdowns", ct.c_int32)]
 
 
+class GilaServerOptsC(ct.Structure):
+    """gila_server_opts (include/gila_b200.h)."""
+    _fields_ = [("hbm_budget", ct.c_int64), ("slots", ct.c_int32), ("ell", ct.c_int32), ("mixed", ct.c_int32),
+                ("int_ord", ct.c_int32), ("frq_re", ct.c_double), ("frq_im", ct.c_double)]
+
+
+class GilaServerStatsC(ct.Structure):
+    """gila_server_stats (include/gila_b200.h)."""
+    _fields_ = [("submitted", ct.c_int64), ("completed", ct.c_int64), ("queued", ct.c_int64),
+                ("running", ct.c_int64), ("batches", ct.c_int64), ("operators", ct.c_int64),
+                ("bytes_in_use", ct.c_int64), ("hbm_budget", ct.c_int64)]
+
+
 _lib = None
 
 # (name, restype, argtypes)
@@ -91,6 +104,13 @@ _SIGS = [
     ("gila_ls_solve", ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,
                                  ct.POINTER(GilaSolveC), ct.POINTER(GilaSolveInfoC), ct.POINTER(ct.c_double),
                                  ct.c_void_p]),
+    ("gila_server_create", ct.c_int, [ct.c_void_p, ct.POINTER(GilaServerOptsC), ct.POINTER(ct.c_void_p)]),
+    ("gila_server_destroy", ct.c_int, [ct.c_void_p]),
+    ("gila_server_submit", ct.c_int, [ct.c_void_p, ct.POINTER(GilaVolC), ct.c_void_p, ct.c_void_p, ct.c_void_p,
+                                      ct.POINTER(GilaSolveC), ct.POINTER(ct.c_uint64)]),
+    ("gila_server_wait", ct.c_int, [ct.c_void_p, ct.c_uint64, ct.c_int64, ct.POINTER(GilaSolveInfoC),
+                                    ct.POINTER(ct.c_double)]),
+    ("gila_server_stats_get", ct.c_int, [ct.c_void_p, ct.POINTER(GilaServerStatsC)]),
     ("gila_opr_apply_noalloc", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p,
                                           ct.c_int64, ct.c_void_p]),
 ]

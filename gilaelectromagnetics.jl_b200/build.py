@@ -18,8 +18,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgila_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["gila.cu", "matvec.cu", "noalloc.cu", "kerbuild.cu", "solver.cu"]
-HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "internal.h"]
+SOURCES = ["gila.cu", "matvec.cu", "noalloc.cu", "kerbuild.cu", "solver.cu", "server.cu"]
+HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "internal.h", "solver.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",

@@ -31,6 +31,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "solver.h"
 
 namespace gila {
 namespace {
@@ -349,15 +350,17 @@ __global__ void __launch_bounds__(kT) k_mr_update(KVec<C> v, int ell, int64_t n,
 }
 
 // Lippmann-Schwinger combine after out = G in: out = in - chi .* out, chi per
-// cell broadcast over the three components (examples/GilaOperators.jl:94).
+// cell broadcast over the three components (examples/GilaOperators.jl:94);
+// chi_rs = 0: one medium for all right-hand sides, V: one per right-hand side.
 template <typename C>
 __global__ void __launch_bounds__(kT) k_ls_combine(const C* __restrict__ in, C* __restrict__ out,
-                                                   const C* __restrict__ chi, int64_t V,
+                                                   const C* __restrict__ chi, int64_t chi_rs, int64_t V,
                                                    const Stat* __restrict__ st) {
   const int r = blockIdx.y;
   if (st && !st[r].act) return;
   in += 3 * V * r;
   out += 3 * V * r;
+  chi += chi_rs * r;
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < V; i += (int64_t)gridDim.x * kT) {
     const double2 c = to_d(chi[i]);
 #pragma unroll
@@ -372,10 +375,12 @@ __global__ void __launch_bounds__(kT) k_ls_combine(const C* __restrict__ in, C* 
 // r = b - (x - chi .* t) with t = G x held in r on entry; partial |r|^2
 // (masked right-hand sides only when mask is set).
 __global__ void __launch_bounds__(kT) k_resid(const double2* __restrict__ b, const double2* __restrict__ x,
-                                              double2* __restrict__ r, const double2* __restrict__ chi, int64_t V,
-                                              const int* __restrict__ mask, double2* __restrict__ part) {
+                                              double2* __restrict__ r, const double2* __restrict__ chi,
+                                              int64_t chi_rs, int64_t V, const int* __restrict__ mask,
+                                              double2* __restrict__ part) {
   const int q = blockIdx.y, nb = gridDim.x;
   if (mask && !mask[q]) return;
+  chi += chi_rs * q;
   const int64_t off = 3 * V * q;
   double2 acc[1] = {make_double2(0.0, 0.0)};
   for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < V; i += (int64_t)nb * kT) {
@@ -492,11 +497,6 @@ struct DevArena {  // frees what it allocated when the solve returns
   }
 };
 
-struct Opts {
-  double tol, delta;
-  int ell, mixed, max_mv, max_restarts, x0, graph;
-};
-
 // blocks per right-hand side of the vector kernels: a function of n only, so
 // that the reduction order never depends on the batch
 int vec_blocks(int64_t n) {
@@ -504,336 +504,632 @@ int vec_blocks(int64_t n) {
   return (int)std::max<int64_t>(1, std::min<int64_t>(b, 1024));
 }
 
-template <typename C>
-cudaError_t ls_apply(Core& c, const C* chi, const C* in, C* out, int nrhs, const Stat* st, int nbv,
-                     cudaStream_t s) {
-  C one, zero;
-  one.x = 1;
-  one.y = 0;
-  zero.x = 0;
-  zero.y = 0;
-  cudaError_t e = launch_matvec<C>(c.geom, devop<C>(c), c.launch, in, out, static_cast<C*>(c.A),
-                                   static_cast<C*>(c.B), nrhs, false, one, zero, s);
-  if (e != cudaSuccess) return e;
-  const int64_t V = in_elems(c) / 3;
-  k_ls_combine<C><<<dim3(nbv, nrhs), kT, 0, s>>>(in, out, chi, V, st);
-  return cudaGetLastError();
+// partial of |a_r|^2 for the masked right-hand sides
+__global__ void __launch_bounds__(kT) k_norm2(const double2* __restrict__ a, int64_t n, const int* __restrict__ mask,
+                                              double2* __restrict__ part) {
+  const int r = blockIdx.y, nb = gridDim.x;
+  if (!mask[r]) return;
+  a += n * r;
+  double2 acc[1] = {make_double2(0.0, 0.0)};
+  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT) acc[0].x += cabs2(a[i]);
+  block_sum_store<1>(acc, 1, part + (int64_t)r * nb + blockIdx.x, nb);
 }
 
-// One batched solve.  Per right-hand side r the host keeps |b|, the FP64
-// residual norm, the scale s of the current Krylov process and the largest
-// recursive residual since the last reliable update; the device keeps the
-// Krylov vectors, the scalars and the status (act / broke / nrm2).
+// maximal runs [r0, r1) of set entries of m
+std::vector<std::pair<int, int>> runs_of(const std::vector<char>& m, int cap) {
+  std::vector<std::pair<int, int>> out;
+  const int S = (int)m.size();
+  for (int r0 = 0; r0 < S;) {
+    if (!m[r0]) {
+      ++r0;
+      continue;
+    }
+    int r1 = r0 + 1;
+    while (r1 < S && m[r1] && r1 - r0 < cap) ++r1;
+    out.emplace_back(r0, r1);
+    r0 = r1;
+  }
+  return out;
+}
+
+template <typename C>
+struct OpRef {  // an operator with workspaces owned by a batch
+  Core* core;
+  Geom geom;    // max_rhs = the workspace capacity
+  C* A;
+  C* B;
+  int cap;      // right-hand sides per matvec launch sequence
+};
+
+// right-hand sides the FP64 workspace of a mixed batch holds: reliable
+// updates are rare, so their matvecs run in chunks
+constexpr int kUpdateCap = 4;
+
 template <typename CI>
-struct Solver {
-  Core& g64;
-  Core& gi;  // Krylov operator (g64 itself when plain)
-  const double2* chi64;
-  const CI* chii;
-  const double2* b;
-  double2* x;
-  int nrhs;
-  int64_t n;
-  Opts o;
-  cudaStream_t s;
-  int nb;
-  DevArena mem;
-  double2 *r64 = nullptr, *part = nullptr, *sc = nullptr;
-  Stat *st_d = nullptr, *st_h = nullptr;
-  // parameter block [tol2 | scale | inv | nrm] doubles then [mask] ints,
-  // mirrored in pinned host memory
-  char *pb_d = nullptr, *pb_h = nullptr;
-  KVec<CI> kv{};
-  CI* shadow = nullptr;
-  cudaGraphExec_t graph = nullptr;
-  bool graph_ok = true;
-  gila_solve_info info{};
-
-  Solver(Core& a, Core& i, const double2* c64, const CI* ci, const double2* bb, double2* xx, int nr, const Opts& oo,
-         cudaStream_t ss)
-      : g64(a), gi(i), chi64(c64), chii(ci), b(bb), x(xx), nrhs(nr), n(in_elems(a)), o(oo), s(ss) {
-    nb = vec_blocks(n);
+class LsBatchT final : public LsBatch {
+ public:
+  LsBatchT(Core& a, Core& i, int S, const BatchCfg& c)
+      : g64_(a), gi_(i), S_(S), n_(in_elems(a)), V_(in_elems(a) / 3), cfg_(c), sl_(S) {
+    nb_ = vec_blocks(n_);
   }
-  ~Solver() {
-    if (graph) cudaGraphExecDestroy(graph);
+  ~LsBatchT() override {
+    if (s_) cudaStreamSynchronize(s_);
+    if (graph_) cudaGraphExecDestroy(graph_);
+    if (ev_) cudaEventDestroy(ev_);
+    mem_.release();
+    if (s_) cudaStreamDestroy(s_);
   }
-  double* pd(int k) const { return reinterpret_cast<double*>(pb_d) + (size_t)k * nrhs; }
-  double* ph(int k) const { return reinterpret_cast<double*>(pb_h) + (size_t)k * nrhs; }
-  int* mask_d() const { return reinterpret_cast<int*>(pb_d + 4 * sizeof(double) * nrhs); }
-  int* mask_h() const { return reinterpret_cast<int*>(pb_h + 4 * sizeof(double) * nrhs); }
-  size_t pb_bytes() const { return (4 * sizeof(double) + sizeof(int)) * (size_t)nrhs; }
 
-  cudaError_t setup() {
-    cudaError_t e;
-    const size_t vb = (size_t)nrhs * n;
-    if ((e = mem.alloc((void**)&r64, vb * sizeof(double2))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&part, (size_t)nrhs * kGram * nb * sizeof(double2))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&sc, (size_t)nrhs * kSlots * sizeof(double2))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&st_d, (size_t)nrhs * sizeof(Stat))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&pb_d, pb_bytes())) != cudaSuccess) return e;
-    if ((e = mem.alloc_host((void**)&st_h, (size_t)nrhs * sizeof(Stat))) != cudaSuccess) return e;
-    if ((e = mem.alloc_host((void**)&pb_h, pb_bytes())) != cudaSuccess) return e;
-    memset(pb_h, 0, pb_bytes());
-    memset(st_h, 0, (size_t)nrhs * sizeof(Stat));
+  static size_t bytes(const Core& a, const Core& i, int S, const BatchCfg& c) {
+    const int64_t n = in_elems(a), V = n / 3;
+    const bool mixed = c.mixed != 0;
+    size_t t = 0;
+    t += 3ull * S * n * sizeof(double2);                                 // b, x, r (FP64)
+    t += (c.chi_shared ? 1ull : (size_t)S) * V * sizeof(double2);        // chi
+    if (mixed) t += (c.chi_shared ? 1ull : (size_t)S) * V * sizeof(CI);  // chi, inner precision
+    t += (size_t)(2 * c.ell + 3) * S * n * sizeof(CI) + n * sizeof(CI);  // Krylov vectors, shadow
+    t += (size_t)S * (kGram * vec_blocks(n) + kSlots) * sizeof(double2) + (size_t)S * (sizeof(Stat) + 64);
+    Geom g = a.geom;
+    g.max_rhs = mixed ? std::min(S, kUpdateCap) : S;
+    Work w = work_sizes(g);
+    t += (size_t)(w.a_elems + w.b_rhs * g.max_rhs) * sizeof(double2);
+    if (mixed) {
+      Geom gi = i.geom;
+      gi.max_rhs = S;
+      gi.csize = sizeof(CI);
+      w = work_sizes(gi);
+      t += (size_t)(w.a_elems + w.b_rhs * S) * sizeof(CI);
+    }
+    return t;
+  }
+
+  gila_status init() {
+    GILA_CUDA_TRY(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    GILA_CUDA_TRY(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
+    const size_t vb = (size_t)S_ * n_;
+    const bool mixed = cfg_.mixed != 0;
+    const int nchi = cfg_.chi_shared ? 1 : S_;
+    GILA_CUDA_TRY(mem_.alloc((void**)&b64_, vb * sizeof(double2)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&x64_, vb * sizeof(double2)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&r64_, vb * sizeof(double2)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&chi64_, (size_t)nchi * V_ * sizeof(double2)));
+    if (mixed)
+      GILA_CUDA_TRY(mem_.alloc((void**)&chii_, (size_t)nchi * V_ * sizeof(CI)));
+    else
+      chii_ = reinterpret_cast<CI*>(chi64_);
+    GILA_CUDA_TRY(mem_.alloc((void**)&part_, (size_t)S_ * kGram * nb_ * sizeof(double2)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&sc_, (size_t)S_ * kSlots * sizeof(double2)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&st_d_, (size_t)S_ * sizeof(Stat)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&pb_d_, pb_bytes()));
+    GILA_CUDA_TRY(mem_.alloc_host((void**)&st_h_, (size_t)S_ * sizeof(Stat)));
+    GILA_CUDA_TRY(mem_.alloc_host((void**)&pb_h_, pb_bytes()));
+    memset(st_h_, 0, (size_t)S_ * sizeof(Stat));
+    memset(pb_h_, 0, pb_bytes());
+    const int nvec = 2 * cfg_.ell + 3;
     CI* base = nullptr;
-    const int nvec = 2 * o.ell + 3;
-    if ((e = mem.alloc((void**)&base, (size_t)nvec * vb * sizeof(CI))) != cudaSuccess) return e;
-    if ((e = mem.alloc((void**)&shadow, (size_t)n * sizeof(CI))) != cudaSuccess) return e;
-    kv.x = base;
-    for (int k = 0; k <= o.ell; ++k) {
-      kv.r[k] = base + (size_t)(1 + k) * vb;
-      kv.u[k] = base + (size_t)(2 + o.ell + k) * vb;
+    GILA_CUDA_TRY(mem_.alloc((void**)&base, (size_t)nvec * vb * sizeof(CI)));
+    GILA_CUDA_TRY(mem_.alloc((void**)&shadow_, (size_t)n_ * sizeof(CI)));
+    kv_.x = base;
+    for (int k = 0; k <= cfg_.ell; ++k) {
+      kv_.r[k] = base + (size_t)(1 + k) * vb;
+      kv_.u[k] = base + (size_t)(2 + cfg_.ell + k) * vb;
     }
-    for (int k = o.ell + 1; k <= kMaxEll; ++k) kv.r[k] = kv.u[k] = nullptr;
-    kv.shadow = shadow;
-    // every Krylov vector starts finite, including those of right-hand sides
-    // that never iterate (their matvecs still run inside the batch)
-    if ((e = cudaMemsetAsync(base, 0, (size_t)nvec * vb * sizeof(CI), s)) != cudaSuccess) return e;
-    if ((e = cudaMemcpyAsync(st_d, st_h, (size_t)nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-      return e;
-    k_shadow<CI><<<nb, kT, 0, s>>>(shadow, n, 0x5EEDull);
-    return cudaGetLastError();
+    for (int k = cfg_.ell + 1; k <= kMaxEll; ++k) kv_.r[k] = kv_.u[k] = nullptr;
+    kv_.shadow = shadow_;
+    // workspaces of the two operators (owned here: batches run concurrently)
+    op64_.core = &g64_;
+    op64_.geom = g64_.geom;
+    op64_.cap = mixed ? std::min(S_, kUpdateCap) : S_;
+    op64_.geom.max_rhs = op64_.cap;
+    {
+      const Work w = work_sizes(op64_.geom);
+      GILA_CUDA_TRY(mem_.alloc((void**)&op64_.A, (size_t)w.a_elems * sizeof(double2)));
+      GILA_CUDA_TRY(mem_.alloc((void**)&op64_.B, (size_t)w.b_rhs * op64_.cap * sizeof(double2)));
+    }
+    if (mixed) {
+      opi_.core = &gi_;
+      opi_.geom = gi_.geom;
+      opi_.cap = S_;
+      opi_.geom.max_rhs = S_;
+      const Work w = work_sizes(opi_.geom);
+      GILA_CUDA_TRY(mem_.alloc((void**)&opi_.A, (size_t)w.a_elems * sizeof(CI)));
+      GILA_CUDA_TRY(mem_.alloc((void**)&opi_.B, (size_t)w.b_rhs * S_ * sizeof(CI)));
+    } else {
+      opi_.core = &gi_;
+      opi_.geom = op64_.geom;
+      opi_.cap = op64_.cap;
+      opi_.A = reinterpret_cast<CI*>(op64_.A);
+      opi_.B = reinterpret_cast<CI*>(op64_.B);
+    }
+    // every Krylov vector starts finite
+    GILA_CUDA_TRY(cudaMemsetAsync(base, 0, (size_t)nvec * vb * sizeof(CI), s_));
+    GILA_CUDA_TRY(cudaMemcpyAsync(st_d_, st_h_, (size_t)S_ * sizeof(Stat), cudaMemcpyHostToDevice, s_));
+    k_shadow<CI><<<nb_, kT, 0, s_>>>(shadow_, n_, 0x5EEDull);
+    GILA_CUDA_TRY(cudaGetLastError());
+    GILA_CUDA_TRY(cudaStreamSynchronize(s_));
+    return GILA_OK;
   }
 
-  // squared norms of the nrhs vectors whose partials are in `part` -> host
-  cudaError_t fetch_norms(std::vector<double>& out) {
-    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, pd(0), FIN_NORM, pd(3));
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if ((e = cudaMemcpyAsync(ph(3), pd(3), nrhs * sizeof(double), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
-      return e;
-    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-    out.assign(ph(3), ph(3) + nrhs);
-    return cudaSuccess;
+  int slots() const override { return S_; }
+  int free_slot() const override {
+    for (int r = 0; r < S_; ++r)
+      if (sl_[r].state == 0) return r;
+    return -1;
+  }
+  int busy_slots() const override {
+    int k = 0;
+    for (const auto& q : sl_) k += q.state != 0;
+    return k;
+  }
+  bool in_flight() const override { return in_flight_; }
+  bool ready() override {
+    if (!in_flight_) return true;
+    const cudaError_t e = cudaEventQuery(ev_);
+    if (e == cudaErrorNotReady) return false;
+    if (e != cudaSuccess) cudaGetLastError();
+    in_flight_ = false;
+    return true;
+  }
+  gila_status wait() override {
+    if (!in_flight_) return GILA_OK;
+    GILA_CUDA_TRY(cudaEventSynchronize(ev_));
+    in_flight_ = false;
+    return GILA_OK;
+  }
+  std::vector<SlotResult> take_finished() override {
+    std::vector<SlotResult> o;
+    o.swap(finished_);
+    return o;
+  }
+  const gila_solve_info& info() const override { return inf_; }
+  cudaStream_t stream() const override { return s_; }
+
+  gila_status set_shared_chi(const void* chi) override {
+    if (!cfg_.chi_shared) return fail(GILA_ERR_ARG, "the batch has one medium per slot");
+    if (in_flight_) return fail(GILA_ERR_INTERNAL, "batch busy");
+    return load_chi(0, chi);
   }
 
-  // r64 = b - A64 x for the right-hand sides set in mask_h (all when null):
-  // one batched FP64 matvec per run of consecutive masked right-hand sides.
-  // Returns |r|^2 per right-hand side (entries of unmasked ones undefined).
-  cudaError_t true_residual(std::vector<double>& rn2, const int* mh) {
-    cudaError_t e;
-    const double2 one = make_double2(1, 0), zero = make_double2(0, 0);
-    for (int r0 = 0; r0 < nrhs;) {
-      if (mh && !mh[r0]) {
-        ++r0;
-        continue;
+  gila_status assign(int r, const void* chi, const void* b, void* x_out, const SlotOpts& o, uint64_t tag) override {
+    if (r < 0 || r >= S_ || sl_[r].state != 0) return fail(GILA_ERR_ARG, "slot is not free");
+    if (in_flight_) return fail(GILA_ERR_INTERNAL, "batch busy");
+    if (!b || !x_out || (!cfg_.chi_shared && !chi)) return fail(GILA_ERR_ARG, "null argument");
+    gila_status st;
+    if (!cfg_.chi_shared && (st = load_chi(r, chi)) != GILA_OK) return st;
+    GILA_CUDA_TRY(cudaMemcpyAsync(b64_ + (size_t)r * n_, b, n_ * sizeof(double2), cudaMemcpyDefault, s_));
+    if (o.x0)
+      GILA_CUDA_TRY(cudaMemcpyAsync(x64_ + (size_t)r * n_, x_out, n_ * sizeof(double2), cudaMemcpyDefault, s_));
+    else
+      GILA_CUDA_TRY(cudaMemsetAsync(x64_ + (size_t)r * n_, 0, n_ * sizeof(double2), s_));
+    Slot& q = sl_[r];
+    q = Slot{};
+    q.state = 1;
+    q.fresh = true;
+    q.o = o;
+    q.x_out = x_out;
+    q.tag = tag;
+    st_h_[r] = Stat{0.0, 0, 0};
+    return GILA_OK;
+  }
+
+  gila_status advance(bool* enq) override {
+    *enq = false;
+    if (in_flight_) return fail(GILA_ERR_INTERNAL, "advance with a step in flight");
+    gila_status st = GILA_OK;
+    // slots whose solution copy has completed are released
+    for (int r = 0; r < S_; ++r)
+      if (sl_[r].state == 2) {
+        sl_[r].state = 0;
+        finished_.push_back(sl_[r].res);
       }
-      int r1 = r0 + 1;
-      while (r1 < nrhs && (!mh || mh[r1])) ++r1;
-      e = launch_matvec<double2>(g64.geom, devop<double2>(g64), g64.launch, x + (size_t)r0 * n, r64 + (size_t)r0 * n,
-                                 static_cast<double2*>(g64.A), static_cast<double2*>(g64.B), r1 - r0, false, one,
-                                 zero, s);
-      if (e != cudaSuccess) return e;
-      r0 = r1;
+    switch (ph_) {
+      case Ph::Init:
+        digest_init();
+        break;
+      case Ph::Cycle: {
+        bool upd = false;
+        if ((st = digest_cycle(&upd)) != GILA_OK) return st;
+        if (upd) return record(enq, Ph::Update);
+        break;
+      }
+      case Ph::Update:
+        if ((st = digest_update()) != GILA_OK) return st;
+        break;
+      default:
+        break;
     }
-    k_resid<<<dim3(nb, nrhs), kT, 0, s>>>(b, x, r64, chi64, n / 3, mh ? mask_d() : nullptr, part);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    ++info.matvecs_f64;
-    return fetch_norms(rn2);
+    bool any_fresh = false, any_iter = false, any_copy = false;
+    for (const auto& q : sl_) {
+      any_fresh |= q.state == 1 && q.fresh;
+      any_copy |= q.state == 2;
+    }
+    if (any_fresh) {
+      if ((st = enqueue_init()) != GILA_OK) return st;
+      return record(enq, Ph::Init);
+    }
+    if ((st = enqueue_starts()) != GILA_OK) return st;
+    for (const auto& q : sl_) any_iter |= q.state == 1 && q.iter;
+    if (any_iter) {
+      if ((st = enqueue_cycle()) != GILA_OK) return st;
+      return record(enq, Ph::Cycle);
+    }
+    for (const auto& q : sl_) any_copy |= q.state == 2;
+    if (any_copy) return record(enq, Ph::Idle);
+    ph_ = Ph::Idle;
+    return GILA_OK;
   }
 
-  // Reliable update of the masked right-hand sides (mask_h set by the
-  // caller): x64 += s d, d = 0, FP64 residual, r_0 = r64 / s.
-  cudaError_t reliable_update(std::vector<double>& rn2) {
-    cudaError_t e;
-    if ((e = cudaMemcpyAsync(pb_d, pb_h, pb_bytes(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
-    k_accum<CI><<<dim3(nb, nrhs), kT, 0, s>>>(x, kv.x, pd(1), mask_d(), n);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = true_residual(rn2, mask_h())) != cudaSuccess) return e;
-    k_replace<CI><<<dim3(nb, nrhs), kT, 0, s>>>(r64, kv.r[0], pd(2), mask_d(), n);
-    ++info.outer;
-    return cudaGetLastError();
+ private:
+  enum class Ph { Idle, Init, Cycle, Update };
+  struct Slot {
+    int state = 0;  // 0 free, 1 assigned, 2 solution copy in flight
+    bool fresh = false;       // norms of b not yet known
+    bool need_start = false;  // (re)start the Krylov process from r64
+    bool iter = false;        // Krylov process running
+    bool pending = false;     // the Krylov iterate holds a correction not yet in x64
+    bool broke = false;
+    bool in_upd = false;      // part of the reliable update in flight
+    double bn = 0, rn = 0, scale = 0, maxr = 0;
+    int restarts = 0, cycles = 0, updates = 0, mv = 0;
+    SlotOpts o;
+    void* x_out = nullptr;
+    uint64_t tag = 0;
+    SlotResult res{};
+  };
+
+  size_t pb_bytes() const { return (5 * sizeof(double) + sizeof(int)) * (size_t)S_; }
+  double* pd(int k) const { return reinterpret_cast<double*>(pb_d_) + (size_t)k * S_; }
+  double* ph(int k) const { return reinterpret_cast<double*>(pb_h_) + (size_t)k * S_; }
+  int* mask_d() const { return reinterpret_cast<int*>(pb_d_ + 5 * sizeof(double) * S_); }
+  int* mask_h() const { return reinterpret_cast<int*>(pb_h_ + 5 * sizeof(double) * S_); }
+  int64_t chi_rs() const { return cfg_.chi_shared ? 0 : V_; }
+  bool done(const Slot& q) const { return q.bn == 0.0 || q.rn <= q.o.tol * q.bn; }
+
+  gila_status record(bool* enq, Ph p) {
+    GILA_CUDA_TRY(cudaEventRecord(ev_, s_));
+    in_flight_ = true;
+    ph_ = p;
+    *enq = true;
+    return GILA_OK;
   }
 
-  // One BiCGStab(l) cycle for every active right-hand side, ending with the
-  // copy of the per-rhs status to the host.
-  cudaError_t body() {
-    cudaError_t e;
-    const dim3 gv(nb, nrhs);
-    const int sb = (nrhs + 127) / 128;
+  gila_status load_chi(int r, const void* chi) {
+    double2* c64 = chi64_ + (size_t)r * V_;
+    GILA_CUDA_TRY(cudaMemcpyAsync(c64, chi, V_ * sizeof(double2), cudaMemcpyDefault, s_));
+    if (cfg_.mixed) {
+      k_cast<CI><<<vec_blocks(V_), kT, 0, s_>>>(c64, chii_ + (size_t)r * V_, V_);
+      GILA_CUDA_TRY(cudaGetLastError());
+    }
+    return GILA_OK;
+  }
+
+  gila_status upload_params() {
+    GILA_CUDA_TRY(cudaMemcpyAsync(pb_d_, pb_h_, pb_bytes(), cudaMemcpyHostToDevice, s_));
+    return GILA_OK;
+  }
+  gila_status upload_status() {
+    GILA_CUDA_TRY(cudaMemcpyAsync(st_d_, st_h_, (size_t)S_ * sizeof(Stat), cudaMemcpyHostToDevice, s_));
+    return GILA_OK;
+  }
+
+  // squared norms (partials in part_) -> pd(k) -> ph(k) after the step
+  gila_status fin_norms(int k) {
+    k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, pd(0), FIN_NORM, pd(k));
+    GILA_CUDA_TRY(cudaGetLastError());
+    GILA_CUDA_TRY(cudaMemcpyAsync(ph(k), pd(k), S_ * sizeof(double), cudaMemcpyDeviceToHost, s_));
+    return GILA_OK;
+  }
+
+  template <typename C>
+  gila_status apply_runs(const OpRef<C>& op, const C* in, C* out, const std::vector<char>& m) {
+    C one, zero;  // host side: no device helpers here
+    one.x = 1;
+    one.y = 0;
+    zero.x = 0;
+    zero.y = 0;
+    for (auto [r0, r1] : runs_of(m, op.cap)) {
+      GILA_CUDA_TRY(launch_matvec<C>(op.geom, devop<C>(*op.core), op.core->launch, in + (size_t)r0 * n_,
+                                     out + (size_t)r0 * n_, op.A, op.B, r1 - r0, false, one, zero, s_));
+    }
+    return GILA_OK;
+  }
+
+  // r64 = b - A64 x64 for the slots in m, squared norms into pd(3) -> ph(3)
+  gila_status true_residual(const std::vector<char>& m) {
+    gila_status st;
+    if ((st = apply_runs<double2>(op64_, x64_, r64_, m)) != GILA_OK) return st;
+    k_resid<<<dim3(nb_, S_), kT, 0, s_>>>(b64_, x64_, r64_, chi64_, chi_rs(), V_, mask_d(), part_);
+    GILA_CUDA_TRY(cudaGetLastError());
+    ++inf_.matvecs_f64;
+    return fin_norms(3);
+  }
+
+  void finish(int r, bool converged) {
+    Slot& q = sl_[r];
+    q.iter = false;
+    q.need_start = false;
+    st_h_[r].act = 0;
+    q.res = SlotResult{r, q.tag, q.bn == 0.0 ? 0.0 : q.rn / q.bn, converged ? 1 : 0, q.cycles, q.updates,
+                       q.broke ? 1 : 0};
+    cudaMemcpyAsync(q.x_out, x64_ + (size_t)r * n_, n_ * sizeof(double2), cudaMemcpyDefault, s_);
+    q.state = 2;
+  }
+
+  // fresh slots: |b|^2 (pd(4)), and for an initial guess r = b - A x (pd(3))
+  gila_status enqueue_init() {
+    int* mh = mask_h();
+    std::vector<char> mx(S_, 0);
+    bool any_x0 = false;
+    for (int r = 0; r < S_; ++r) {
+      const Slot& q = sl_[r];
+      mh[r] = q.state == 1 && q.fresh;
+      mx[r] = mh[r] && q.o.x0;
+      any_x0 |= mx[r] != 0;
+      if (mh[r] && !q.o.x0)
+        GILA_CUDA_TRY(cudaMemcpyAsync(r64_ + (size_t)r * n_, b64_ + (size_t)r * n_, n_ * sizeof(double2),
+                                      cudaMemcpyDeviceToDevice, s_));
+    }
+    gila_status st;
+    if ((st = upload_params()) != GILA_OK) return st;
+    k_norm2<<<dim3(nb_, S_), kT, 0, s_>>>(b64_, n_, mask_d(), part_);
+    GILA_CUDA_TRY(cudaGetLastError());
+    if ((st = fin_norms(4)) != GILA_OK) return st;
+    if (any_x0) {
+      // the residual of the initial guesses, for those slots only
+      for (int r = 0; r < S_; ++r) mh[r] = mx[r];
+      if ((st = upload_params()) != GILA_OK) return st;
+      if ((st = true_residual(mx)) != GILA_OK) return st;
+    }
+    return GILA_OK;
+  }
+
+  void digest_init() {
+    for (int r = 0; r < S_; ++r) {
+      Slot& q = sl_[r];
+      if (!(q.state == 1 && q.fresh)) continue;
+      q.fresh = false;
+      q.bn = std::sqrt(ph(4)[r]);
+      q.rn = q.o.x0 ? std::sqrt(ph(3)[r]) : q.bn;
+      if (done(q))
+        finish(r, true);
+      else if (!std::isfinite(q.rn))
+        finish(r, false);
+      else
+        q.need_start = true;
+    }
+  }
+
+  gila_status enqueue_starts() {
+    int* mh = mask_h();
+    int nstart = 0;
+    for (int r = 0; r < S_; ++r) {
+      Slot& q = sl_[r];
+      mh[r] = 0;
+      if (q.state != 1 || !q.need_start) continue;
+      q.need_start = false;
+      ++q.restarts;
+      q.iter = true;
+      q.scale = q.rn;
+      q.maxr = 1.0;
+      st_h_[r] = Stat{1.0, 1, 0};
+      mh[r] = 1;
+      ++nstart;
+    }
+    if (!nstart) return GILA_OK;
+    for (int r = 0; r < S_; ++r) {
+      const Slot& q = sl_[r];
+      const bool live = q.state == 1 && q.iter;
+      const double t = live ? 0.9 * q.o.tol * q.bn / q.scale : 0.0;
+      ph(0)[r] = t * t;
+      ph(1)[r] = live ? q.scale : 0.0;
+      ph(2)[r] = live ? 1.0 / q.scale : 0.0;
+    }
+    gila_status st;
+    if ((st = upload_params()) != GILA_OK) return st;
+    if ((st = upload_status()) != GILA_OK) return st;
+    k_inner_start<CI><<<dim3(nb_, S_), kT, 0, s_>>>(r64_, kv_, pd(2), mask_d(), n_);
+    k_scal_init<<<(S_ + 127) / 128, 128, 0, s_>>>(sc_, mask_d(), S_);
+    GILA_CUDA_TRY(cudaGetLastError());
+    return GILA_OK;
+  }
+
+  // One BiCGStab(l) cycle for the slots in `m` (matvecs over their runs; the
+  // vector kernels cover all slots and skip inactive ones), ending with the
+  // copy of the per-slot status to the host.
+  gila_status body(const std::vector<char>& m) {
+    const dim3 gv(nb_, S_);
+    const int sb = (S_ + 127) / 128;
     double* tol2 = pd(0);
-    k_iter_start<<<sb, 128, 0, s>>>(sc, st_d, nrhs);
-    for (int j = 1; j <= o.ell; ++j) {
-      k_dot<CI, CI><<<gv, kT, 0, s>>>(shadow, 0, kv.r[j - 1], n, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_RHO, st_d, tol2, FIN_CHECK);
-      k_bicg_u<CI><<<gv, kT, 0, s>>>(kv, j, n, sc, st_d);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      if ((e = ls_apply<CI>(gi, chii, kv.u[j - 1], kv.u[j], nrhs, st_d, nb, s)) != cudaSuccess) return e;
-      k_dot<CI, CI><<<gv, kT, 0, s>>>(shadow, 0, kv.u[j], n, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, S_SIG, st_d, tol2, FIN_CHECK);
-      k_bicg_r<CI><<<gv, kT, 0, s>>>(kv, j, n, sc, st_d, part);
-      k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2, FIN_RESID);
-      if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      if ((e = ls_apply<CI>(gi, chii, kv.r[j - 1], kv.r[j], nrhs, st_d, nb, s)) != cudaSuccess) return e;
+    gila_status st;
+    const int ell = cfg_.ell;
+    auto lsa = [&](const CI* in, CI* out) -> gila_status {
+      gila_status s2 = apply_runs<CI>(opi_, in, out, m);
+      if (s2 != GILA_OK) return s2;
+      k_ls_combine<CI><<<gv, kT, 0, s_>>>(in, out, chii_, chi_rs(), V_, st_d_);
+      return GILA_OK;
+    };
+    k_iter_start<<<sb, 128, 0, s_>>>(sc_, st_d_, S_);
+    for (int j = 1; j <= ell; ++j) {
+      k_dot<CI, CI><<<gv, kT, 0, s_>>>(shadow_, 0, kv_.r[j - 1], n_, part_);
+      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_RHO, st_d_, tol2, FIN_CHECK);
+      k_bicg_u<CI><<<gv, kT, 0, s_>>>(kv_, j, n_, sc_, st_d_);
+      GILA_CUDA_TRY(cudaGetLastError());
+      if ((st = lsa(kv_.u[j - 1], kv_.u[j])) != GILA_OK) return st;
+      k_dot<CI, CI><<<gv, kT, 0, s_>>>(shadow_, 0, kv_.u[j], n_, part_);
+      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_SIG, st_d_, tol2, FIN_CHECK);
+      k_bicg_r<CI><<<gv, kT, 0, s_>>>(kv_, j, n_, sc_, st_d_, part_);
+      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
+      GILA_CUDA_TRY(cudaGetLastError());
+      if ((st = lsa(kv_.r[j - 1], kv_.r[j])) != GILA_OK) return st;
     }
-    k_gram<CI><<<gv, kT, 0, s>>>(kv, o.ell, n, part);
-    k_fin<<<nrhs, kT, 0, s>>>(part, kGram, nb, sc, S_GRAM, st_d, tol2, FIN_STORE);
-    k_mr_solve<<<sb, 128, 0, s>>>(sc, st_d, o.ell, nrhs);
-    k_mr_update<CI><<<gv, kT, 0, s>>>(kv, o.ell, n, sc, st_d, part);
-    k_fin<<<nrhs, kT, 0, s>>>(part, 1, nb, sc, 0, st_d, tol2, FIN_RESID);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    return cudaMemcpyAsync(st_h, st_d, nrhs * sizeof(Stat), cudaMemcpyDeviceToHost, s);
+    k_gram<CI><<<gv, kT, 0, s_>>>(kv_, ell, n_, part_);
+    k_fin<<<S_, kT, 0, s_>>>(part_, kGram, nb_, sc_, S_GRAM, st_d_, tol2, FIN_STORE);
+    k_mr_solve<<<sb, 128, 0, s_>>>(sc_, st_d_, ell, S_);
+    k_mr_update<CI><<<gv, kT, 0, s_>>>(kv_, ell, n_, sc_, st_d_, part_);
+    k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
+    GILA_CUDA_TRY(cudaGetLastError());
+    GILA_CUDA_TRY(cudaMemcpyAsync(st_h_, st_d_, (size_t)S_ * sizeof(Stat), cudaMemcpyDeviceToHost, s_));
+    return GILA_OK;
   }
 
-  cudaError_t iterate(bool first) {
-    if (o.graph && graph_ok && !graph && !first) {
-      // the first cycle ran directly (function attributes are set); capture the next
+  gila_status enqueue_cycle() {
+    std::vector<char> m(S_, 0);
+    for (int r = 0; r < S_; ++r) m[r] = sl_[r].state == 1 && sl_[r].iter;
+    std::vector<int> key;
+    for (auto [r0, r1] : runs_of(m, S_)) {
+      key.push_back(r0);
+      key.push_back(r1);
+    }
+    // a pattern of iterating slots seen twice in a row is captured once and
+    // replayed; the first cycle of a pattern runs directly (it also sets the
+    // kernels' function attributes outside any capture)
+    if (cfg_.graph && graph_ok_ && key != graph_key_ && key == last_key_) {
+      if (graph_) {
+        cudaGraphExecDestroy(graph_);
+        graph_ = nullptr;
+      }
       cudaGraph_t g = nullptr;
-      cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+      cudaError_t e = cudaStreamBeginCapture(s_, cudaStreamCaptureModeThreadLocal);
       if (e == cudaSuccess) {
-        cudaError_t eb = body();
-        e = cudaStreamEndCapture(s, &g);
-        if (eb == cudaSuccess && e == cudaSuccess && g) e = cudaGraphInstantiate(&graph, g, 0);
+        const gila_status sb = body(m);
+        e = cudaStreamEndCapture(s_, &g);
+        if (sb == GILA_OK && e == cudaSuccess && g) e = cudaGraphInstantiate(&graph_, g, 0);
         if (g) cudaGraphDestroy(g);
-        if (eb != cudaSuccess || e != cudaSuccess) {
-          graph = nullptr;
-          graph_ok = false;
+        if (sb != GILA_OK || e != cudaSuccess) {
+          graph_ = nullptr;
+          graph_ok_ = false;
+        } else {
+          graph_key_ = key;
         }
       } else {
-        graph_ok = false;
+        graph_ok_ = false;
       }
       cudaGetLastError();
     }
-    if (graph) return cudaGraphLaunch(graph, s);
-    return body();
+    last_key_ = key;
+    ++inf_.iters;
+    if (cfg_.mixed)
+      inf_.matvecs_f32 += 2 * cfg_.ell;
+    else
+      inf_.matvecs_f64 += 2 * cfg_.ell;
+    if (graph_ && key == graph_key_) {
+      GILA_CUDA_TRY(cudaGraphLaunch(graph_, s_));
+      return GILA_OK;
+    }
+    return body(m);
   }
 
-  cudaError_t run(std::vector<double>& res) {
-    cudaError_t e;
-    const size_t vb = (size_t)nrhs * n;
-    std::vector<double> bn2, rn2;
-    k_dot<double2, double2><<<dim3(nb, nrhs), kT, 0, s>>>(b, n, b, n, part);
-    if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    if ((e = fetch_norms(bn2)) != cudaSuccess) return e;
-    if (o.x0) {
-      if ((e = true_residual(rn2, nullptr)) != cudaSuccess) return e;
-    } else {
-      if ((e = cudaMemsetAsync(x, 0, vb * sizeof(double2), s)) != cudaSuccess) return e;
-      if ((e = cudaMemcpyAsync(r64, b, vb * sizeof(double2), cudaMemcpyDeviceToDevice, s)) != cudaSuccess) return e;
-      rn2 = bn2;
-    }
-    std::vector<double> bn(nrhs), rn(nrhs), scale(nrhs, 0.0), maxr(nrhs, 0.0);
-    std::vector<char> live(nrhs, 0), restart(nrhs, 0), broke(nrhs, 0), pending(nrhs, 0);
-    std::vector<int> restarts(nrhs, 0);
-    for (int r = 0; r < nrhs; ++r) {
-      bn[r] = std::sqrt(bn2[r]);
-      rn[r] = std::sqrt(rn2[r]);
-    }
-    auto done = [&](int r) { return bn[r] == 0.0 || rn[r] <= o.tol * bn[r]; };
-    for (int r = 0; r < nrhs; ++r) restart[r] = !done(r) && std::isfinite(rn[r]);
-    const double delta = o.mixed ? o.delta : 0.0;
-    const int mv_iter = 2 * o.ell;
-    int mv = 0;
+  // after a cycle: per slot, a reliable update on breakdown, claimed
+  // convergence, an exhausted matvec budget or (mixed) a recursive residual
+  // below delta times its largest value since the last update
+  gila_status digest_cycle(bool* upd) {
+    *upd = false;
+    const bool mixed = cfg_.mixed != 0;
     int* mh = mask_h();
-    for (;;) {
-      // (re)start the Krylov processes that need it, on A d = r / |r|
-      int nstart = 0;
-      for (int r = 0; r < nrhs; ++r) {
-        mh[r] = 0;
-        if (!restart[r]) continue;
-        restart[r] = 0;
-        if (restarts[r] >= o.max_restarts) continue;
-        ++restarts[r];
+    std::vector<char> m(S_, 0);
+    const int mvc = 2 * cfg_.ell;
+    for (int r = 0; r < S_; ++r) {
+      Slot& q = sl_[r];
+      mh[r] = 0;
+      q.in_upd = false;
+      if (!(q.state == 1 && q.iter)) continue;
+      ++q.cycles;
+      q.mv += mvc;
+      q.pending = true;
+      const Stat& s = st_h_[r];
+      const double nr = std::sqrt(s.nrm2);
+      const bool budget = q.mv + mvc > q.o.max_mv;
+      if (s.broke || !s.act || budget || (mixed && nr < q.o.delta * q.maxr)) {
+        m[r] = 1;
         mh[r] = 1;
-        ++nstart;
-        live[r] = 1;
-        scale[r] = rn[r];
-        maxr[r] = 1.0;
-        st_h[r].nrm2 = 1.0;
-        st_h[r].act = 1;
-        st_h[r].broke = 0;
+        q.in_upd = true;
+      } else if (nr > q.maxr) {
+        q.maxr = nr;
       }
-      if (nstart) {
-        for (int r = 0; r < nrhs; ++r) {
-          const double t = live[r] ? 0.9 * o.tol * bn[r] / scale[r] : 0.0;
-          ph(0)[r] = t * t;
-          ph(1)[r] = live[r] ? scale[r] : 0.0;
-          ph(2)[r] = live[r] ? 1.0 / scale[r] : 0.0;
-        }
-        if ((e = cudaMemcpyAsync(pb_d, pb_h, pb_bytes(), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
-        if ((e = cudaMemcpyAsync(st_d, st_h, nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess)
-          return e;
-        k_inner_start<CI><<<dim3(nb, nrhs), kT, 0, s>>>(r64, kv, pd(2), mask_d(), n);
-        k_scal_init<<<(nrhs + 127) / 128, 128, 0, s>>>(sc, mask_d(), nrhs);
-        if ((e = cudaGetLastError()) != cudaSuccess) return e;
-      }
-      int nlive = 0;
-      for (int r = 0; r < nrhs; ++r) nlive += live[r];
-      if (nlive == 0 || mv + mv_iter > o.max_mv) break;
-      // one cycle; its status copy is read after the sync
-      if ((e = iterate(info.iters == 0)) != cudaSuccess) return e;
-      if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
-      mv += mv_iter;
-      ++info.iters;
-      if (o.mixed)
-        info.matvecs_f32 += mv_iter;
-      else
-        info.matvecs_f64 += mv_iter;
-      // reliable updates: breakdown, claimed convergence, or (mixed) a
-      // recursive residual below delta times its largest value since the last
-      int nupd = 0;
-      for (int r = 0; r < nrhs; ++r) {
-        mh[r] = 0;
-        if (!live[r]) continue;
-        pending[r] = 1;
-        const Stat& q = st_h[r];
-        const double nr = std::sqrt(q.nrm2);
-        if (q.broke || !q.act || nr < delta * maxr[r]) {
-          mh[r] = 1;
-          ++nupd;
-        } else if (nr > maxr[r]) {
-          maxr[r] = nr;
-        }
-      }
-      if (nupd == 0) continue;
-      if ((e = reliable_update(rn2)) != cudaSuccess) return e;
-      for (int r = 0; r < nrhs; ++r) {
-        if (!mh[r]) continue;
-        pending[r] = 0;
-        rn[r] = std::sqrt(rn2[r]);
-        Stat& q = st_h[r];
-        broke[r] |= (char)q.broke;
-        if (done(r)) {
-          live[r] = 0;
-          q.act = 0;
-        } else if (q.broke || !q.act || !std::isfinite(rn[r])) {
-          // breakdown, or convergence the FP64 residual does not confirm:
-          // restart from the FP64 residual
-          live[r] = 0;
-          q.act = 0;
-          restart[r] = std::isfinite(rn[r]);
-        } else {
-          maxr[r] = rn[r] / scale[r];
-          q.nrm2 = maxr[r] * maxr[r];
-        }
-      }
-      if ((e = cudaMemcpyAsync(st_d, st_h, nrhs * sizeof(Stat), cudaMemcpyHostToDevice, s)) != cudaSuccess) return e;
     }
-    // fold the corrections still held by the Krylov iterates into x
-    int npend = 0;
-    for (int r = 0; r < nrhs; ++r) {
-      mh[r] = pending[r];
-      npend += pending[r];
-    }
-    if (npend) {
-      if ((e = reliable_update(rn2)) != cudaSuccess) return e;
-      for (int r = 0; r < nrhs; ++r)
-        if (pending[r]) rn[r] = std::sqrt(rn2[r]);
-    }
-    res.resize(nrhs);
-    info.converged = 0;
-    info.rel_res = 0.0;
-    info.breakdowns = 0;
-    for (int r = 0; r < nrhs; ++r) {
-      res[r] = bn[r] == 0.0 ? 0.0 : rn[r] / bn[r];
-      info.rel_res = std::max(info.rel_res, res[r]);
-      if (!std::isfinite(res[r])) info.rel_res = res[r];
-      info.converged += done(r) ? 1 : 0;
-      info.breakdowns += broke[r] ? 1 : 0;
-    }
-    return cudaSuccess;
+    bool any = false;
+    for (char c : m) any |= c != 0;
+    if (!any) return GILA_OK;
+    gila_status st;
+    if ((st = upload_params()) != GILA_OK) return st;
+    k_accum<CI><<<dim3(nb_, S_), kT, 0, s_>>>(x64_, kv_.x, pd(1), mask_d(), n_);
+    GILA_CUDA_TRY(cudaGetLastError());
+    if ((st = true_residual(m)) != GILA_OK) return st;
+    k_replace<CI><<<dim3(nb_, S_), kT, 0, s_>>>(r64_, kv_.r[0], pd(2), mask_d(), n_);
+    GILA_CUDA_TRY(cudaGetLastError());
+    ++inf_.outer;
+    *upd = true;
+    return GILA_OK;
   }
+
+  gila_status digest_update() {
+    const int mvc = 2 * cfg_.ell;
+    for (int r = 0; r < S_; ++r) {
+      Slot& q = sl_[r];
+      if (!q.in_upd) continue;
+      q.in_upd = false;
+      q.pending = false;
+      ++q.updates;
+      q.rn = std::sqrt(ph(3)[r]);
+      Stat& s = st_h_[r];
+      q.broke |= s.broke != 0;
+      if (done(q)) {
+        finish(r, true);
+      } else if (q.mv + mvc > q.o.max_mv || !std::isfinite(q.rn)) {
+        finish(r, false);
+      } else if (s.broke || !s.act) {
+        // breakdown, or convergence the FP64 residual does not confirm:
+        // restart from the FP64 residual
+        q.iter = false;
+        s.act = 0;
+        if (q.restarts >= q.o.max_restarts)
+          finish(r, false);
+        else
+          q.need_start = true;
+      } else {
+        q.maxr = q.rn / q.scale;
+        s.nrm2 = q.maxr * q.maxr;
+      }
+    }
+    return upload_status();
+  }
+
+  Core& g64_;
+  Core& gi_;
+  int S_;
+  int64_t n_, V_;
+  BatchCfg cfg_;
+  int nb_ = 1;
+  cudaStream_t s_ = nullptr;
+  cudaEvent_t ev_ = nullptr;
+  struct Arena : DevArena {
+    void release() {
+      for (void* p : d) cudaFree(p);
+      for (void* p : h) cudaFreeHost(p);
+      d.clear();
+      h.clear();
+    }
+  } mem_;
+  OpRef<double2> op64_{};
+  OpRef<CI> opi_{};
+  double2 *b64_ = nullptr, *x64_ = nullptr, *r64_ = nullptr, *chi64_ = nullptr;
+  CI* chii_ = nullptr;
+  double2 *part_ = nullptr, *sc_ = nullptr;
+  Stat *st_d_ = nullptr, *st_h_ = nullptr;
+  char *pb_d_ = nullptr, *pb_h_ = nullptr;
+  KVec<CI> kv_{};
+  CI* shadow_ = nullptr;
+  cudaGraphExec_t graph_ = nullptr;
+  std::vector<int> graph_key_, last_key_;
+  bool graph_ok_ = true;
+  std::vector<Slot> sl_;
+  Ph ph_ = Ph::Idle;
+  bool in_flight_ = false;
+  gila_solve_info inf_{};
+  std::vector<SlotResult> finished_;
 };
+
+}  // namespace
 
 bool same_volume(const Core& a, const Core& b) {
   for (int k = 0; k < 3; ++k)
@@ -841,6 +1137,46 @@ bool same_volume(const Core& a, const Core& b) {
   return a.geom.parT == b.geom.parT && a.parS == b.parS;
 }
 
+gila_status check_ls_operator(const Core& a) {
+  if (a.dtype != GILA_C128) return fail(GILA_ERR_TYPE, "the residual operator must be ComplexF64");
+  if (!a.self || a.geom.parT != 1 || a.parS != 1 || in_elems(a) != out_elems(a))
+    return fail(GILA_ERR_SIZE, "Green's operator and medium must have the same size (a self operator).");
+  return GILA_OK;
+}
+
+size_t ls_batch_bytes(const Core& g64, const Core* g32, int slots, const BatchCfg& cfg) {
+  if (cfg.mixed && g32) return LsBatchT<float2>::bytes(g64, *g32, slots, cfg);
+  return LsBatchT<double2>::bytes(g64, g64, slots, cfg);
+}
+
+gila_status make_ls_batch(Core& g64, Core* g32, int slots, const BatchCfg& cfg, std::unique_ptr<LsBatch>& out) {
+  gila_status s = check_ls_operator(g64);
+  if (s != GILA_OK) return s;
+  if (slots < 1 || slots > 65535) return fail(GILA_ERR_ARG, "slots must be in 1..65535");
+  if (cfg.ell < 1 || cfg.ell > kMaxEll) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
+  for (Core* c : {&g64, g32}) {
+    if (c && !c->tuned) {
+      c->launch = default_launch(*c);
+      c->tuned = true;
+    }
+  }
+  if (cfg.mixed) {
+    if (!g32) return fail(GILA_ERR_ARG, "the mixed solve needs the ComplexF32 operator");
+    if (g32->dtype != GILA_C64) return fail(GILA_ERR_TYPE, "the inner operator must be ComplexF32");
+    if (!same_volume(g64, *g32) || g32->device != g64.device)
+      return fail(GILA_ERR_SIZE, "the two operators describe different volumes");
+    auto b = std::make_unique<LsBatchT<float2>>(g64, *g32, slots, cfg);
+    if ((s = b->init()) != GILA_OK) return s;
+    out = std::move(b);
+  } else {
+    auto b = std::make_unique<LsBatchT<double2>>(g64, g64, slots, cfg);
+    if ((s = b->init()) != GILA_OK) return s;
+    out = std::move(b);
+  }
+  return GILA_OK;
+}
+
+namespace {
 template <typename C>
 __global__ void k_cast_any(const void* __restrict__ a, int a_f64, C* __restrict__ b, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
@@ -856,21 +1192,12 @@ __global__ void k_cast_any(const void* __restrict__ a, int a_f64, C* __restrict_
 }
 
 }  // namespace
-}  // namespace gila
 
-using namespace gila;
-
-extern "C" {
-
-gila_status gila_opr_cast(gila_opr* opr, gila_dtype dtype, gila_opr** out) {
-  if (!opr || !opr->core || !out) return fail(GILA_ERR_ARG, "null argument");
+gila_status cast_core(gila_ctx* ctx, Core& c, gila_dtype dtype, std::shared_ptr<Core>& core) {
   if (dtype != GILA_C64 && dtype != GILA_C128) return fail(GILA_ERR_TYPE, "setTyp must be ComplexF32 or ComplexF64");
-  Core& c = *opr->core;
-  std::lock_guard<std::mutex> lk(c.mu);
   GILA_CUDA_TRY(cudaSetDevice(c.device));
   const gila_vol trg = vol_to_abi(c.trg), src = vol_to_abi(c.src);
-  std::shared_ptr<Core> core;
-  gila_status s = init_core(opr->ctx, &trg, c.self ? nullptr : &src, &c.opt, dtype, core);
+  gila_status s = init_core(ctx, &trg, c.self ? nullptr : &src, &c.opt, dtype, core);
   if (s != GILA_OK) return s;
   const int64_t elems = (int64_t)(c.ker_bytes / csize(c.dtype));
   core->ker_bytes = (size_t)elems * csize(dtype);
@@ -884,6 +1211,23 @@ gila_status gila_opr_cast(gila_opr* opr, gila_dtype dtype, gila_opr** out) {
                                                       elems);
   GILA_CUDA_TRY(cudaGetLastError());
   GILA_CUDA_TRY(cudaStreamSynchronize(c.stream));
+  return GILA_OK;
+}
+
+}  // namespace gila
+
+using namespace gila;
+
+extern "C" {
+
+gila_status gila_opr_cast(gila_opr* opr, gila_dtype dtype, gila_opr** out) {
+  if (!opr || !opr->core || !out) return fail(GILA_ERR_ARG, "null argument");
+  std::shared_ptr<Core> core;
+  gila_status s;
+  {
+    std::lock_guard<std::mutex> lk(opr->core->mu);
+    if ((s = cast_core(opr->ctx, *opr->core, dtype, core)) != GILA_OK) return s;
+  }
   auto* o = new gila_opr;
   o->ctx = opr->ctx;
   o->core = core;
@@ -899,89 +1243,67 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   if (!g64 || !g64->core || !chi || !b || !x) return fail(GILA_ERR_ARG, "null argument");
   if (nrhs < 1 || nrhs > 65535) return fail(GILA_ERR_ARG, "nrhs must be in 1..65535");
   Core& a = *g64->core;
-  if (a.dtype != GILA_C128) return fail(GILA_ERR_TYPE, "the residual operator must be ComplexF64");
-  if (!a.self || a.geom.parT != 1 || a.parS != 1 || in_elems(a) != out_elems(a))
-    return fail(GILA_ERR_SIZE, "Green's operator and medium must have the same size (a self operator).");
-  Opts o;
-  o.tol = opts && opts->tol > 0 ? opts->tol : 1e-6;
-  o.ell = opts && opts->ell > 0 ? opts->ell : 2;
-  o.mixed = opts ? (opts->mixed != 0) : 0;
-  o.max_mv = opts && opts->max_matvecs > 0 ? opts->max_matvecs : 4000;
-  o.max_restarts = opts && opts->max_restarts > 0 ? opts->max_restarts : 20;
-  o.delta = opts && opts->delta > 0 ? opts->delta : 0.1;
-  o.x0 = opts ? (opts->x0 != 0) : 0;
-  o.graph = opts ? (opts->no_graph == 0) : 1;
+  gila_status s = check_ls_operator(a);
+  if (s != GILA_OK) return s;
+  BatchCfg cfg;
+  SlotOpts so;
+  cfg.ell = opts && opts->ell > 0 ? opts->ell : 2;
+  cfg.mixed = opts ? (opts->mixed != 0) : 0;
+  cfg.graph = opts ? (opts->no_graph == 0) : 1;
+  cfg.chi_shared = 1;
   if (const char* ev = getenv("GILA_SOLVE_GRAPH"))
-    if (ev[0] == '0') o.graph = 0;
-  if (o.ell > kMaxEll) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
-  Core* inner = &a;
-  if (o.mixed) {
+    if (ev[0] == '0') cfg.graph = 0;
+  so.tol = opts && opts->tol > 0 ? opts->tol : 1e-6;
+  so.max_mv = opts && opts->max_matvecs > 0 ? opts->max_matvecs : 4000;
+  so.max_restarts = opts && opts->max_restarts > 0 ? opts->max_restarts : 20;
+  so.delta = opts && opts->delta > 0 ? opts->delta : 0.1;
+  so.x0 = opts ? (opts->x0 != 0) : 0;
+  if (cfg.ell > 4) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
+  Core* inner = nullptr;
+  if (cfg.mixed) {
     if (!g32 || !g32->core) return fail(GILA_ERR_ARG, "the mixed solve needs the ComplexF32 operator");
     inner = g32->core.get();
-    if (inner->dtype != GILA_C64) return fail(GILA_ERR_TYPE, "the inner operator must be ComplexF32");
-    if (!same_volume(a, *inner) || inner->device != a.device)
-      return fail(GILA_ERR_SIZE, "the two operators describe different volumes");
   }
-  std::unique_lock<std::mutex> la(a.mu, std::defer_lock), lb(inner->mu, std::defer_lock);
-  if (inner != &a)
-    std::lock(la, lb);
-  else
-    la.lock();
   GILA_CUDA_TRY(cudaSetDevice(a.device));
-  for (Core* c : {&a, inner}) {
-    gila_status s = ensure_work(*c, nrhs);
-    if (s != GILA_OK) return s;
-    if (!c->tuned) {
-      c->launch = default_launch(*c);
-      c->tuned = true;
-    }
-  }
-  cudaStream_t st = a.stream;
+  std::unique_ptr<LsBatch> bt;
+  if ((s = make_ls_batch(a, inner, (int)nrhs, cfg, bt)) != GILA_OK) return s;
+  cudaStream_t st = bt->stream();
   cudaStream_t user = static_cast<cudaStream_t>(stream);
-  DevArena mem;
   cudaEvent_t ev = nullptr;
   if (user) {
     GILA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     GILA_CUDA_TRY(cudaEventRecord(ev, user));
     GILA_CUDA_TRY(cudaStreamWaitEvent(st, ev, 0));
   }
-  const int64_t n = in_elems(a), V = n / 3, nv = n * nrhs;
-  // device copies of chi, b and x
-  double2 *chi64 = nullptr, *bd = nullptr, *xd = nullptr;
-  GILA_CUDA_TRY(mem.alloc((void**)&chi64, V * sizeof(double2)));
-  GILA_CUDA_TRY(cudaMemcpyAsync(chi64, chi, V * sizeof(double2), cudaMemcpyDefault, st));
-  if (is_device_ptr(b)) {
-    bd = const_cast<double2*>(static_cast<const double2*>(b));
-  } else {
-    GILA_CUDA_TRY(mem.alloc((void**)&bd, nv * sizeof(double2)));
-    GILA_CUDA_TRY(cudaMemcpyAsync(bd, b, nv * sizeof(double2), cudaMemcpyHostToDevice, st));
+  const int64_t n = in_elems(a);
+  if ((s = bt->set_shared_chi(chi)) != GILA_OK) return s;
+  for (int64_t r = 0; r < nrhs; ++r) {
+    const void* br = static_cast<const double2*>(b) + r * n;
+    void* xr = static_cast<double2*>(x) + r * n;
+    if ((s = bt->assign((int)r, nullptr, br, xr, so, (uint64_t)r)) != GILA_OK) return s;
   }
-  GILA_CUDA_TRY(mem.alloc((void**)&xd, nv * sizeof(double2)));
-  if (o.x0) GILA_CUDA_TRY(cudaMemcpyAsync(xd, x, nv * sizeof(double2), cudaMemcpyDefault, st));
-  std::vector<double> res;
-  gila_solve_info inf{};
-  cudaError_t e;
-  if (o.mixed) {
-    float2* chi32 = nullptr;
-    GILA_CUDA_TRY(mem.alloc((void**)&chi32, V * sizeof(float2)));
-    k_cast<float2><<<vec_blocks(V), kT, 0, st>>>(chi64, chi32, V);
-    GILA_CUDA_TRY(cudaGetLastError());
-    Solver<float2> sv(a, *inner, chi64, chi32, bd, xd, (int)nrhs, o, st);
-    if ((e = sv.setup()) != cudaSuccess || (e = sv.run(res)) != cudaSuccess) {
-      cudaStreamSynchronize(st);
-      return cuda_fail(e, "gila_ls_solve");
-    }
-    inf = sv.info;
-  } else {
-    Solver<double2> sv(a, a, chi64, chi64, bd, xd, (int)nrhs, o, st);
-    if ((e = sv.setup()) != cudaSuccess || (e = sv.run(res)) != cudaSuccess) {
-      cudaStreamSynchronize(st);
-      return cuda_fail(e, "gila_ls_solve");
-    }
-    inf = sv.info;
+  for (;;) {
+    bool enq = false;
+    if ((s = bt->advance(&enq)) != GILA_OK) break;
+    if (!enq) break;
+    if ((s = bt->wait()) != GILA_OK) break;
   }
-  GILA_CUDA_TRY(cudaMemcpyAsync(x, xd, nv * sizeof(double2), cudaMemcpyDefault, st));
-  GILA_CUDA_TRY(cudaStreamSynchronize(st));
+  cudaStreamSynchronize(st);
+  if (s != GILA_OK) return s;
+  std::vector<SlotResult> fin = bt->take_finished();
+  gila_solve_info inf = bt->info();
+  inf.converged = 0;
+  inf.breakdowns = 0;
+  inf.rel_res = 0.0;
+  std::vector<double> res(nrhs, 0.0);
+  for (const SlotResult& q : fin) {
+    res[q.slot] = q.rel_res;
+    inf.converged += q.converged;
+    inf.breakdowns += q.broke;
+    inf.rel_res = std::isfinite(inf.rel_res) ? std::max(inf.rel_res, q.rel_res) : inf.rel_res;
+    if (!std::isfinite(q.rel_res)) inf.rel_res = q.rel_res;
+  }
+  if ((int64_t)fin.size() != nrhs) return fail(GILA_ERR_INTERNAL, "a right-hand side was not reported");
   if (ev) {
     cudaEventRecord(ev, st);
     cudaStreamWaitEvent(user, ev, 0);
@@ -992,7 +1314,7 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
     for (int64_t r = 0; r < nrhs; ++r) rhs_res[r] = res[r];
   if (inf.converged < nrhs)
     return fail(GILA_ERR_NOTCONV, "the solve stopped at relative residual " + std::to_string(inf.rel_res) +
-                                      " above the tolerance " + std::to_string(o.tol));
+                                      " above the tolerance " + std::to_string(so.tol));
   return GILA_OK;
 }
 

@@ -208,6 +208,55 @@ typedef struct {
 gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const void* b, void* x, int64_t nrhs,
                           const gila_solve_opts* opts, gila_solve_info* info, double* rhs_res, void* stream);
 
+/* ---- the solve server: continuous batching of scattering solves -------- */
+/* No counterpart in the reference (its solves are single blocking calls).
+ * A server owns one scheduler thread per context.  Requests (a self volume,
+ * its medium chi and incident field b) are queued on submit; the scheduler
+ * keeps one batch of right-hand-side slots per volume shape on its own CUDA
+ * stream, with the shape's ComplexF64 and ComplexF32 operators (built on the
+ * GPU and cached) and all Krylov vectors resident in HBM.  A request joins
+ * its shape's running batch at the next Krylov-cycle boundary as soon as a
+ * slot is free and the HBM budget admits the batch; batches of different
+ * shapes run concurrently on their streams.  Each right-hand side's result
+ * does not depend on what else is batched with it. */
+typedef struct gila_server gila_server;
+
+typedef struct {
+  int64_t hbm_budget;      /* device bytes for operators and batches; 0 -> free memory at
+                              creation minus 4 GiB */
+  int32_t slots;           /* right-hand-side slots of a shape's batch; 0 -> 8 */
+  int32_t ell;             /* BiCGStab(l) degree of every solve; 0 -> 2 */
+  int32_t mixed;           /* ComplexF32 Krylov process with FP64 reliable updates */
+  int32_t int_ord;         /* GlaKerOpt intOrd of the operators built; 0 -> 32 */
+  double frq_re, frq_im;   /* GlaKerOpt frqPhz; 0 + 0i -> 1 + 0i */
+} gila_server_opts;
+
+typedef struct {
+  int64_t submitted, completed, queued, running;
+  int64_t batches;         /* shape batches allocated */
+  int64_t operators;       /* shapes whose operators are cached */
+  int64_t bytes_in_use;    /* operators + batches, device bytes */
+  int64_t hbm_budget;
+} gila_server_stats;
+
+gila_status gila_server_create(gila_ctx* ctx, const gila_server_opts* opts, gila_server** out);
+gila_status gila_server_destroy(gila_server* srv);
+/* vol: a self volume (cells, scale; origin ignored); chi: (Nx,Ny,Nz)
+ * complex128; b, x: (Nx,Ny,Nz,3) complex128 host or device pointers that
+ * stay valid until the request completes (x receives the solution).  opts:
+ * tol, max_matvecs, max_restarts, delta of this request (ell / mixed are the
+ * server's); NULL for defaults. */
+gila_status gila_server_submit(gila_server* srv, const gila_vol* vol, const void* chi, const void* b, void* x,
+                               const gila_solve_opts* opts, uint64_t* ticket);
+/* Wait for a request (timeout_ms < 0: no limit; GILA_ERR_TIMEOUT when it
+ * runs out).  info (may be NULL): that right-hand side's cycles (iters),
+ * reliable updates (outer), rel_res, converged; latency_ms (may be NULL):
+ * submit to completion on the host clock.  Returns GILA_ERR_NOTCONV when the
+ * solve missed its tolerance. */
+gila_status gila_server_wait(gila_server* srv, uint64_t ticket, int64_t timeout_ms, gila_solve_info* info,
+                             double* latency_ms);
+gila_status gila_server_stats_get(gila_server* srv, gila_server_stats* out);
+
 /* A matvec that allocates no device memory.  This entry point has no
  * counterpart in the reference.  It computes out = G * in for one vector,
  * like gila_opr_apply, for callers that cannot let the library call
