@@ -191,6 +191,9 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-requests", type=int, default=40,
+                    help="requests of the Poisson stream and of the burst that measures saturation")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -289,6 +292,8 @@ def main():
         out["sweep"] = sweep(torch, gila, stream, flush, y_dev)
     if not a.no_solve and world == 1:
         out["solve"] = solve_bench(torch, gila)
+    if not a.no_serve and world == 1:
+        out["serve"] = serve_bench(gila, a.serve_requests)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -423,6 +428,95 @@ def solve_bench(torch, gila):
                                    "speedup_mixed_vs_plain": round(msp / msm, 3)}
     del ls, G, xm, xp, B, D
     torch.cuda.empty_cache()
+    return res
+
+
+SERVE_SHAPES = [(32, 32, 32), (64, 64, 64), (96, 96, 48), (128, 128, 64), (192, 192, 96)]
+
+
+def serve_request(cel, rng):
+    """A cube or slab inclusion with chi = U[0.5,4] + i U[0,0.2] and one
+    s-polarised plane wave at a random angle in the xz plane."""
+    chi = np.zeros(cel, dtype=np.complex128, order="F")
+    val = rng.uniform(0.5, 4.0) + 1j * rng.uniform(0.0, 0.2)
+    if rng.random() < 0.5:
+        lo = [n // 4 for n in cel]
+        hi = [n - n // 4 for n in cel]
+        chi[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] = val
+    else:
+        z0 = cel[2] // 3
+        chi[:, :, z0:cel[2] - z0] = val
+    th = rng.uniform(0.0, math.pi)
+    h = 1.0 / 32
+    x = np.arange(cel[0]) * h
+    z = np.arange(cel[2]) * h
+    ph = np.exp(2j * math.pi * (math.sin(th) * x[:, None, None] + math.cos(th) * z[None, None, :]))
+    b = np.zeros((*cel, 3), dtype=np.complex128, order="F")
+    b[..., 1] = np.broadcast_to(ph, cel)
+    return chi, b
+
+
+def serve_bench(gila, n_stream):
+    """The request stream: solves of volumes drawn uniformly from
+    SERVE_SHAPES (1/32-wavelength cells), each with its own medium and
+    incident wave, tol 1e-6, ComplexF32 Krylov with FP64 reliable updates.
+    A burst of n_stream requests (submitted at once) measures the saturation
+    throughput; then n_stream requests drawn the same way arrive as a Poisson
+    process at 80% of it (seeded).
+    Inputs come from a pool of 3 seeded variants per shape."""
+    rng = np.random.default_rng(11)
+    pool = {c: [serve_request(c, rng) for _ in range(3)] for c in SERVE_SHAPES}
+    srv = gila.SolveServer(slots=8, mixed=True)
+    res = {"shapes": ["x".join(map(str, c)) for c in SERVE_SHAPES], "tol": 1e-6}
+    try:
+        # operators (built on the GPU) and one solve per shape, alone
+        alone = {}
+        for c in SERVE_SHAPES:
+            t0 = time.perf_counter()
+            _, inf, lat = srv.wait(srv.submit(c, SCL, *pool[c][0]))
+            alone["x".join(map(str, c))] = {"first_ms_incl_build": round((time.perf_counter() - t0) * 1e3, 1)}
+            _, inf, lat = srv.wait(srv.submit(c, SCL, *pool[c][0]))
+            alone["x".join(map(str, c))].update({"ms": round(lat, 1), "cycles": inf.iters})
+        res["alone"] = alone
+        # saturation: a burst
+        nb = max(4, n_stream)
+        picks = [SERVE_SHAPES[i] for i in rng.integers(0, len(SERVE_SHAPES), nb)]
+        t0 = time.perf_counter()
+        tk = [srv.submit(c, SCL, *pool[c][int(rng.integers(0, 3))]) for c in picks]
+        for t in tk:
+            srv.wait(t)
+        sat = nb / (time.perf_counter() - t0)
+        res["saturation_solves_per_s"] = round(sat, 3)
+        # Poisson stream at 80% of saturation
+        lam = 0.8 * sat
+        picks = [SERVE_SHAPES[i] for i in rng.integers(0, len(SERVE_SHAPES), n_stream)]
+        gaps = rng.exponential(1.0 / lam, n_stream)
+        tk = []
+        t_start = time.perf_counter()
+        t_next = t_start
+        for c, g in zip(picks, gaps):
+            t_next += g
+            d = t_next - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tk.append((c, srv.submit(c, SCL, *pool[c][int(rng.integers(0, 3))])))
+        lats, conv = [], 0
+        per = {}
+        for c, t in tk:
+            _, inf, lat = srv.wait(t)
+            lats.append(lat)
+            conv += inf.converged
+            per.setdefault("x".join(map(str, c)), []).append(lat)
+        wall = time.perf_counter() - t_start
+        lats = np.array(lats)
+        res.update({
+            "requests": n_stream, "arrival_rate_per_s": round(lam, 3), "solves_per_s": round(n_stream / wall, 3),
+            "p50_ms": round(float(np.percentile(lats, 50)), 1), "p99_ms": round(float(np.percentile(lats, 99)), 1),
+            "mean_ms": round(float(lats.mean()), 1), "converged": conv,
+            "p50_ms_by_shape": {k: round(float(np.median(v)), 1) for k, v in per.items()},
+            "server": srv.stats()})
+    finally:
+        srv.close()
     return res
 
 
