@@ -329,6 +329,24 @@ class GlaOprMem:
         _check(L.lib().gila_opr_time_passes(self._h, int(nrhs), int(reps), ms))
         return tuple(ms)
 
+    def autotune(self, nrhs: int = 1):
+        """Time the compiled tile candidates for nrhs vectors and keep the
+        fastest; returns (x-forward lines, x-inverse lines, y tile, z tile)."""
+        t = (ct.c_int32 * 4)()
+        _check(L.lib().gila_opr_autotune(self._h, int(nrhs), t))
+        return tuple(t)
+
+    @property
+    def tiles(self):
+        t = (ct.c_int32 * 4)()
+        _check(L.lib().gila_opr_get_tiles(self._h, t))
+        return tuple(t)
+
+    @tiles.setter
+    def tiles(self, v):
+        t = (ct.c_int32 * 4)(*[int(a) for a in v])
+        _check(L.lib().gila_opr_set_tiles(self._h, t))
+
     def launches_per_apply(self, nrhs: int = 1) -> int:
         n = ct.c_int64()
         _check(L.lib().gila_opr_launches_per_apply(self._h, int(nrhs), ct.byref(n)))

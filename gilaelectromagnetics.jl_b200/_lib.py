@@ -9,7 +9,9 @@ import ctypes as ct
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libgila_b200.so")
+# GILA_B200_LIB names another build of the same library (a debug build, a build
+# with other compile-time options)
+LIB_PATH = os.environ.get("GILA_B200_LIB") or os.path.join(HERE, "libgila_b200.so")
 
 GILA_OK = 0
 GILA_ERR_ARG = 1
@@ -99,6 +101,9 @@ _SIGS = [
     ("gila_opr_reserve", ct.c_int, [ct.c_void_p, ct.c_int64]),
     ("gila_opr_device_bytes", ct.c_int, [ct.c_void_p, ct.POINTER(ct.c_int64)]),
     ("gila_opr_time_passes", ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int, ct.c_double * 4]),
+    ("gila_opr_autotune", ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int32 * 4]),
+    ("gila_opr_get_tiles", ct.c_int, [ct.c_void_p, ct.c_int32 * 4]),
+    ("gila_opr_set_tiles", ct.c_int, [ct.c_void_p, ct.c_int32 * 4]),
     ("gila_opr_launches_per_apply", ct.c_int, [ct.c_void_p, ct.c_int64, ct.POINTER(ct.c_int64)]),
     ("gila_opr_cast", ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]),
     ("gila_ls_solve", ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,

@@ -12,14 +12,16 @@ import argparse
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgila_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["gila.cu", "matvec.cu", "noalloc.cu", "kerbuild.cu", "solver.cu", "server.cu"]
-HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "internal.h", "solver.h"]
+SOURCES = ["gila.cu", "matvec.cu", "matvec_c128.cu", "matvec_c64.cu", "noalloc.cu", "kerbuild.cu", "solver.cu",
+           "server.cu"]
+HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "matvec_impl.cuh", "internal.h", "solver.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
@@ -42,28 +44,30 @@ def _stale(out: str, deps) -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False, extra_flags=None) -> str:
+def build(force: bool = False, verbose: bool = False, extra_flags=None, out: str = LIB,
+          objdir: str | None = None) -> str:
     srcs = [os.path.join(CSRC, s) for s in SOURCES]
     deps = srcs + [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INCLUDE, "gila_b200.h")]
-    if not force and not _stale(LIB, deps):
-        return LIB
-    objdir = os.path.join(HERE, "_build")
+    if not force and not _stale(out, deps):
+        return out
+    objdir = objdir or os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
     nvcc = _nvcc()
     flags = NVCC_FLAGS + list(extra_flags or [])
-    for s in srcs:
-        o = os.path.join(objdir, os.path.basename(s) + ".o")
-        cmd = [nvcc, *flags, "-I", INCLUDE, "-c", s, "-o", o]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
-        objs.append(o)
-    cmd = [nvcc, *flags, "-shared", "-o", LIB, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+    objs = [os.path.join(objdir, os.path.basename(s) + ".o") for s in srcs]
+    cmds = [[nvcc, *flags, "-I", INCLUDE, "-c", s, "-o", o] for s, o in zip(srcs, objs)]
+    if verbose:
+        for c in cmds:
+            print(" ".join(c), flush=True)
+    # the translation units compile in parallel
+    with ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for r in ex.map(lambda c: subprocess.run(c, check=True), cmds):
+            pass
+    cmd = [nvcc, *flags, "-shared", "-o", out, *objs, "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
-    return LIB
+    return out
 
 
 if __name__ == "__main__":

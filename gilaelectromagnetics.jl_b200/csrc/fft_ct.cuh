@@ -58,12 +58,26 @@ constexpr int ct_span(int P, int s) {
   return ns;
 }
 constexpr bool ct_supported(int P) { return ct_odd(P) == 1 || ct_odd(P) == 3 || ct_odd(P) == 5 || ct_odd(P) == 9; }
+// the same radices in reverse order (REV): the inverse transform of the z
+// pass starts with the radix the forward transform ends with, so that the
+// forward's last stage, the 3x3 multiply and the inverse's first stage run on
+// the same registers
+template <bool REV>
+constexpr int ct_radix_o(int P, int s) {
+  return REV ? ct_radix(P, ct_nst(P) - 1 - s) : ct_radix(P, s);
+}
+template <bool REV>
+constexpr int ct_span_o(int P, int s) {
+  int ns = 1;
+  for (int k = 0; k < s; ++k) ns *= ct_radix_o<REV>(P, k);
+  return ns;
+}
 
 // One stage; T = threads per CTA, M = lines.
-template <typename C, int P, int S, int E, int T, int M, bool INV, bool LINE_FAST, class Ld, class St>
+template <typename C, int P, int S, int E, int T, int M, bool INV, bool LINE_FAST, bool REV, class Ld, class St>
 __device__ __forceinline__ void ct_stage(const C* __restrict__ tw, const Ld& ld, const St& st, bool sync_mid) {
-  constexpr int R = ct_radix(P, S);
-  constexpr int NS = ct_span(P, S);
+  constexpr int R = ct_radix_o<REV>(P, S);
+  constexpr int NS = ct_span_o<REV>(P, S);
   constexpr int TPL = P / R;
   constexpr int NTASK = M * TPL;
   constexpr int K = (NTASK + T - 1) / T;
@@ -112,32 +126,35 @@ __device__ __forceinline__ void ct_stage(const C* __restrict__ tw, const Ld& ld,
   }
 }
 
-template <typename C, int P, int S, int E, int T, int M, bool INV, bool LINE_FAST, class LdF, class LdM, class StM,
-          class StL>
-__device__ __forceinline__ void ct_run_from(const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
-                                            const StM& st_mid, const StL& st_last, bool first_in_smem,
-                                            bool last_in_smem) {
-  if constexpr (S < ct_nst(P)) {
-    constexpr bool first = (S == 0), last = (S == ct_nst(P) - 1);
+// stages [S0, S1) of the schedule (S runs from S0); ld_first feeds stage
+// S0, st_last takes the output of stage S1 - 1
+template <typename C, int P, int S0, int S, int S1, int E, int T, int M, bool INV, bool LINE_FAST, bool REV,
+          class LdF, class LdM, class StM, class StL>
+__device__ __forceinline__ void ct_run_range(const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
+                                             const StM& st_mid, const StL& st_last, bool first_in_smem,
+                                             bool last_in_smem) {
+  if constexpr (S < S1) {
+    constexpr bool first = (S == S0), last = (S == S1 - 1);
     const bool sync_mid = (first ? first_in_smem : true) && (last ? last_in_smem : true);
     if constexpr (first && last)
-      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_first, st_last, sync_mid);
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST, REV>(tw, ld_first, st_last, sync_mid);
     else if constexpr (first)
-      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_first, st_mid, sync_mid);
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST, REV>(tw, ld_first, st_mid, sync_mid);
     else if constexpr (last)
-      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_mid, st_last, sync_mid);
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST, REV>(tw, ld_mid, st_last, sync_mid);
     else
-      ct_stage<C, P, S, E, T, M, INV, LINE_FAST>(tw, ld_mid, st_mid, sync_mid);
+      ct_stage<C, P, S, E, T, M, INV, LINE_FAST, REV>(tw, ld_mid, st_mid, sync_mid);
     __syncthreads();
-    ct_run_from<C, P, S + 1, E, T, M, INV, LINE_FAST>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem,
-                                                      last_in_smem);
+    ct_run_range<C, P, S0, S + 1, S1, E, T, M, INV, LINE_FAST, REV>(tw, ld_first, ld_mid, st_mid, st_last,
+                                                                     first_in_smem, last_in_smem);
   }
 }
 
 template <typename C, int P, int E, int T, int M, bool INV, bool LINE_FAST, class LdF, class LdM, class StM, class StL>
 __device__ __forceinline__ void ct_run(const C* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
                                        const StM& st_mid, const StL& st_last, bool first_in_smem, bool last_in_smem) {
-  ct_run_from<C, P, 0, E, T, M, INV, LINE_FAST>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem, last_in_smem);
+  ct_run_range<C, P, 0, 0, ct_nst(P), E, T, M, INV, LINE_FAST, false>(tw, ld_first, ld_mid, st_mid, st_last,
+                                                                      first_in_smem, last_in_smem);
 }
 
 // ---------------------------------------------------------- launch shapes
@@ -165,6 +182,15 @@ constexpr int ct_ztile(int P) {
 constexpr int ct_threads(int M, int P) {
   int t = ct_round32((M * P + 7) / 8);
   return t < 32 ? 32 : t;
+}
+// tile widths the y and z kernels are instantiated for (the autotuner picks
+// among them per operator): at most 512 threads and the shared-memory budget
+constexpr int kTileSet[3] = {4, 8, 16};
+constexpr bool ct_y_ok(int CS, int P, int TX) {
+  return ct_threads(TX, P) <= 512 && (long long)TX * P * CS <= 200 * 1024;
+}
+constexpr bool ct_z_ok(int CS, int P, int TX) {
+  return ct_threads(TX, P) <= 512 && 3LL * TX * P * CS <= 100 * 1024;
 }
 
 }  // namespace gila

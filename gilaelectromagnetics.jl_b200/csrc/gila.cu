@@ -448,9 +448,147 @@ gila_status ensure_work(Core& c, int64_t nrhs) {
   return GILA_OK;
 }
 
+void release_work(Core& c) {
+  cudaFree(c.A);
+  cudaFree(c.B);
+  c.A = c.B = nullptr;
+  c.cap_rhs = 0;
+}
+
 int64_t in_elems(const Core& c) { return 3LL * c.geom.sc[0] * c.geom.sc[1] * c.geom.sc[2]; }
 int64_t out_elems(const Core& c) {
   return 3LL * c.geom.out_full[0] * c.geom.out_full[1] * c.geom.out_full[2];
+}
+
+// ------------------------------------------------------------ autotuner
+// Tile widths of the y and z passes (kx per CTA) are picked per operator
+// geometry, precision and batch size by timing every compiled candidate on
+// the operator's own workspaces; results are cached per context.  The tile
+// does not change any arithmetic (each line's transform and each point's
+// multiply are the same), only the launch shape.
+static std::string tune_key(const Core& c, int64_t nrhs) {
+  const Geom& g = c.geom;
+  char b[256];
+  snprintf(b, sizeof b, "%d|%d,%d,%d|%d,%d,%d|%d,%d,%d|%d|%lld", (int)c.dtype, g.P[0], g.P[1], g.P[2], g.sc[0],
+           g.sc[1], g.sc[2], g.tc[0], g.tc[1], g.tc[2], g.parT, (long long)nrhs);
+  return b;
+}
+
+template <typename C>
+static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
+  const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
+  C *din = nullptr, *dout = nullptr;
+  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
+  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
+  if (e != cudaSuccess) {
+    cudaFree(din);
+    return cuda_fail(e, "cudaMalloc");
+  }
+  cudaMemsetAsync(din, 0, (size_t)ni * sizeof(C), c.stream);
+  cudaEvent_t ev[2];
+  cudaEventCreate(&ev[0]);
+  cudaEventCreate(&ev[1]);
+  const DevOp<C> d = devop<C>(c);
+  C one, zero;
+  one.x = 1;
+  one.y = 0;
+  zero.x = 0;
+  zero.y = 0;
+  // device ms of the given phases, best of 3 after a warm-up
+  auto time_of = [&](const Launch& L, std::initializer_list<int> phases) -> float {
+    float bt = 1e30f;
+    for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
+      cudaEventRecord(ev[0], c.stream);
+      for (int ph : phases) {
+        e = launch_matvec_phase<C>(ph, c.geom, d, L, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B),
+                                   (int)nrhs, false, one, zero, c.stream);
+        if (e != cudaSuccess) break;
+      }
+      cudaEventRecord(ev[1], c.stream);
+      cudaEventSynchronize(ev[1]);
+      float t = 0;
+      cudaEventElapsedTime(&t, ev[0], ev[1]);
+      if (r > 0 && t < bt) bt = t;
+    }
+    return bt;
+  };
+  const int cs = (int)csize(c.dtype);
+  best = default_launch(c);
+  std::vector<int> zc = ct_tiles(cs, c.geom.P[2], true), yc = ct_tiles(cs, c.geom.P[1], false);
+  if (zc.size() > 1) {
+    float bt = 1e30f;
+    int pick = best.z_tx;
+    for (int tx : zc) {
+      Launch L = best;
+      L.z_tx = tx;
+      const float t = time_of(L, {1});
+      if (e != cudaSuccess) break;
+      if (t < bt) {
+        bt = t;
+        pick = tx;
+      }
+    }
+    best.z_tx = pick;
+  }
+  if (yc.size() > 1 && e == cudaSuccess) {
+    float bt = 1e30f;
+    int pick = best.y_tx;
+    for (int tx : yc) {
+      Launch L = best;
+      L.y_tx = tx;
+      const float t = time_of(L, {0, 2});
+      if (e != cudaSuccess) break;
+      if (t < bt) {
+        bt = t;
+        pick = tx;
+      }
+    }
+    best.y_tx = pick;
+  }
+  cudaEventDestroy(ev[0]);
+  cudaEventDestroy(ev[1]);
+  cudaFree(din);
+  cudaFree(dout);
+  if (e != cudaSuccess) return cuda_fail(e, "autotune");
+  return GILA_OK;
+}
+
+gila_status autotune(Core& c, int64_t nrhs) {
+  gila_status s = ensure_work(c, nrhs);
+  if (s != GILA_OK) return s;
+  Launch L;
+  if (c.dtype == GILA_C128)
+    s = tune_t<double2>(c, nrhs, L);
+  else
+    s = tune_t<float2>(c, nrhs, L);
+  if (s != GILA_OK) return s;
+  c.launch = L;
+  c.tuned = true;
+  std::lock_guard<std::mutex> lk(c.ctx->mu);
+  c.ctx->tune_cache[tune_key(c, nrhs)] = L;
+  return GILA_OK;
+}
+
+// The launch shapes of the first use: the context's cached choice for this
+// geometry, else a tuning run (GILA_AUTOTUNE=0: the defaults).
+gila_status ensure_tuned(Core& c, int64_t nrhs) {
+  if (c.tuned) return GILA_OK;
+  {
+    std::lock_guard<std::mutex> lk(c.ctx->mu);
+    auto it = c.ctx->tune_cache.find(tune_key(c, nrhs));
+    if (it != c.ctx->tune_cache.end()) {
+      c.launch = it->second;
+      c.tuned = true;
+      return GILA_OK;
+    }
+  }
+  const char* ev = getenv("GILA_AUTOTUNE");
+  if (ev && ev[0] == '0') {
+    c.launch = default_launch(c);
+    c.tuned = true;
+    return GILA_OK;
+  }
+  return autotune(c, nrhs);
 }
 
 template <typename C>
@@ -460,10 +598,7 @@ static gila_status apply_t(Core& c, const void* in, void* out, int64_t nrhs, boo
   const size_t cs = sizeof(C);
   gila_status s = ensure_work(c, nrhs);
   if (s != GILA_OK) return s;
-  if (!c.tuned) {
-    c.launch = default_launch(c);
-    c.tuned = true;
-  }
+  if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
   cudaStream_t st = user_st ? user_st : c.stream;
   const bool din = is_device_ptr(in), dout = is_device_ptr(out);
   // element alignment (the passes copy with 16 / 8 byte cp.async)
@@ -530,10 +665,7 @@ template <typename C>
 gila_status time_passes_t(Core& c, int64_t nrhs, int reps, double ms[4]) {
   gila_status s = ensure_work(c, nrhs);
   if (s != GILA_OK) return s;
-  if (!c.tuned) {
-    c.launch = default_launch(c);
-    c.tuned = true;
-  }
+  if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
   C *din = nullptr, *dout = nullptr;
   GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
@@ -778,11 +910,50 @@ gila_status gila_opr_reserve(gila_opr* opr, int64_t nrhs) {
   Core& c = *opr->core;
   std::lock_guard<std::mutex> lk(c.mu);
   GILA_CUDA_TRY(cudaSetDevice(c.device));
-  if (!c.tuned) {
-    c.launch = default_launch(c);
-    c.tuned = true;
+  gila_status s = ensure_work(c, nrhs);
+  if (s != GILA_OK) return s;
+  return ensure_tuned(c, nrhs);
+}
+
+gila_status gila_opr_autotune(gila_opr* opr, int64_t nrhs, int32_t tiles[4]) {
+  if (!opr || nrhs < 1) return fail(GILA_ERR_ARG, "invalid argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  GILA_CUDA_TRY(cudaSetDevice(c.device));
+  gila_status s = autotune(c, nrhs);
+  if (s != GILA_OK) return s;
+  if (tiles) {
+    tiles[0] = c.launch.xf_lines;
+    tiles[1] = c.launch.xi_lines;
+    tiles[2] = c.launch.y_tx;
+    tiles[3] = c.launch.z_tx;
   }
-  return ensure_work(c, nrhs);
+  return GILA_OK;
+}
+
+gila_status gila_opr_get_tiles(gila_opr* opr, int32_t tiles[4]) {
+  if (!opr || !tiles) return fail(GILA_ERR_ARG, "null argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  const Launch L = c.tuned ? c.launch : default_launch(c);
+  tiles[0] = L.xf_lines;
+  tiles[1] = L.xi_lines;
+  tiles[2] = L.y_tx;
+  tiles[3] = L.z_tx;
+  return GILA_OK;
+}
+
+gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]) {
+  if (!opr || !tiles) return fail(GILA_ERR_ARG, "null argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  Launch L = c.tuned ? c.launch : default_launch(c);
+  const int cs = (int)csize(c.dtype);
+  if (tiles[2] > 0) L.y_tx = ct_tile_pick(cs, c.geom.P[1], tiles[2], false) == tiles[2] ? tiles[2] : L.y_tx;
+  if (tiles[3] > 0) L.z_tx = ct_tile_pick(cs, c.geom.P[2], tiles[3], true) == tiles[3] ? tiles[3] : L.z_tx;
+  c.launch = L;
+  c.tuned = true;
+  return GILA_OK;
 }
 
 gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes) {

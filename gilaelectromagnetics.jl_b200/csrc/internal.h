@@ -93,6 +93,10 @@ Launch default_launch(const Core& c);
 // GPU FP64 Fourier-kernel build into c.ker (kerbuild.cu)
 gila_status build_kernel(Core& c);
 gila_status ensure_work(Core& c, int64_t nrhs);
+void release_work(Core& c);  // frees the matvec workspaces (allocated again on demand)
+// launch shapes: cached per context, else timed (autotune) at first use
+gila_status ensure_tuned(Core& c, int64_t nrhs);
+gila_status autotune(Core& c, int64_t nrhs);
 int64_t in_elems(const Core& c);
 int64_t out_elems(const Core& c);
 bool is_device_ptr(const void* p);

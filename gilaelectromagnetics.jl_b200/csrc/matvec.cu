@@ -26,21 +26,13 @@
 
 namespace gila {
 
-// complex values staged per thread per FFT stage: power-of-two plans (radix
-// 2/4/8 only) and mixed plans (radix 3/5/7 too) are separate instantiations
-// so that the common case carries no register pressure from the odd radices.
-#ifndef GILA_KE_MIXED
-#define GILA_KE_MIXED 4
-#endif
-constexpr int kE = 8;
-constexpr int kEm = GILA_KE_MIXED;
-template <bool MX> struct StageE { static constexpr int v = MX ? kEm : kE; };
-
-// Shared-memory row of an x pass: element i sits at i + i/8, which spreads
-// the stride-R accesses of the early Stockham stages over all banks.
-__host__ __device__ __forceinline__ int row_stride(int P) { return P + (P + 7) / 8; }
-
 static inline int round_up(int a, int b) { return (a + b - 1) / b * b; }
+
+static bool is_mixed_plan(const AxisPlan& pl) {
+  for (int s = 0; s < pl.nst; ++s)
+    if (pl.radix[s] != 2 && pl.radix[s] != 4 && pl.radix[s] != 8) return true;
+  return false;
+}
 
 Work work_sizes(const Geom& g) {
   const int64_t slab_bytes = g.slab_bytes > 0 ? g.slab_bytes : kSlabBytes;
@@ -67,848 +59,10 @@ int smem_optin_bytes() {
   return v;
 }
 
-// -------------------------------------------------------------------- xfwd
-template <typename C>
-struct XfParams {
-  const C* in;
-  C* A;
-  const AxisPlan* pl;  // device copy
-  int P;
-  const C* tw;
-  int nin;       // source x cells
-  int M;         // rows per CTA
-  int64_t rows;  // total rows = 3 * sy * sz * nrhs
-  FDiv nind;     // division by nin
-};
-
-template <typename C, bool MX>
-__global__ void __launch_bounds__(512) k_xfwd(const XfParams<C> p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const AxisPlan* const pl = p.pl;
-  const int P = p.P, M = p.M, nin = p.nin;
-  const int64_t rows = p.rows;
-  C* const A = p.A;
-  const int64_t g0 = (int64_t)blockIdx.x * M;
-  const int LS = row_stride(P);
-  // stage the M input rows (nin values each) into shared memory
-  {
-    const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
-    const C* const src = p.in + g0 * nin;
-    for (int q = threadIdx.x; q < nl * nin; q += blockDim.x) {
-      const int l = (int)p.nind.div((uint32_t)q);
-      const int i = q - l * nin;
-      cp_async(sm + l * LS + i + (i >> 3), src + q);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  auto ldf = [=](int l, int i) -> C {
-    if (i < nin) return sm[l * LS + i + (i >> 3)];
-    return czero<C>();
-  };
-  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
-  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
-  auto stg = [=](int l, int i, C v) {
-    const int64_t g = g0 + l;
-    if (g < rows) A[g * P + i] = v;
-  };
-  const FDiv md{1, 0, 0};  // unused: rows are not the fastest task index
-  fft_run<C, StageE<MX>::v, false, false, MX>(pl, M, md, p.tw, ldf, lds, sts, stg, true, false);
-}
-
-// ---------------------------------------------------------------------- y
-template <typename C>
-struct YParams {
-  const C* src;
-  C* dst;
-  const AxisPlan* pl;  // device copy
-  int P;
-  const C* tw;
-  int Px;
-  int TX;
-  int ntiles;     // ceil(Px / TX)
-  int nin, nout;  // rows read / written
-  int nz;         // z planes per channel in this pass
-  int src_z, dst_z;          // z planes per channel in the src / dst layouts
-  int src_rows, dst_rows;    // y rows per plane in the src / dst layouts
-  int64_t q0;                // first plane (ch*nz + z) of this launch
-  int64_t src_sub, dst_sub;  // plane index of the first plane held by src / dst
-  FDiv md;                   // division by the line count TX
-};
-
-template <typename C, bool INV, bool MX>
-__global__ void __launch_bounds__(512) k_y(const YParams<C> p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const AxisPlan* const pl = p.pl;
-  const int Px = p.Px, TX = p.TX, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
-  const int64_t rc = slice / p.nz;
-  const int z = (int)(slice % p.nz);
-  const int kx0 = tile * TX;
-  const int M = TX;
-  const C* const src = p.src + ((rc * p.src_z + z) - p.src_sub) * p.src_rows * (int64_t)Px + kx0;
-  C* const dst = p.dst + ((rc * p.dst_z + z) - p.dst_sub) * p.dst_rows * (int64_t)Px + kx0;
-  const int tmax = Px - kx0;
-  // stage the TX x nin input tile into shared memory [i][t]
-  for (int q = threadIdx.x; q < nin * TX; q += blockDim.x) {
-    const int i = (int)p.md.div((uint32_t)q);
-    const int t = q - i * TX;
-    if (t < tmax) cp_async(sm + q, src + (int64_t)i * Px + t);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  auto ldf = [=](int t, int i) -> C {
-    if (t < tmax && i < nin) return sm[i * M + t];
-    return czero<C>();
-  };
-  auto lds = [=](int t, int i) -> C { return sm[i * M + t]; };
-  auto sts = [=](int t, int i, C v) { sm[i * M + t] = v; };
-  auto stg = [=](int t, int i, C v) {
-    if (t < tmax && i < nout) dst[(int64_t)i * Px + t] = v;
-  };
-  fft_run<C, StageE<MX>::v, INV, true, MX>(pl, M, p.md, p.tw, ldf, lds, sts, stg, true, false);
-}
-
-// ---------------------------------------------------------------------- z
-// Kernel address of frequency f on one axis (mirror rules of mulBrnDev!,
-// src/glaActSup.jl:789-846), computed arithmetically: branch bit p = f & 1,
-// stored index m, mirrored flag (sign flip of the off-diagonal components).
-struct AxMap {
-  int brn;   // P / 2
-  int full;  // stored extent == brn (no mirror)
-  int fe;    // forward count of the even branch: ceil(t/2) + iseven(t)
-  int fo;    // forward count of the odd branch: ceil(t/2)
-};
-__device__ __forceinline__ void ax_map(const AxMap& a, int f, int& p, int& m, int& mir) {
-  p = f & 1;
-  const int k = f >> 1;
-  if (a.full) {
-    m = k;
-    mir = 0;
-  } else if (p == 0) {
-    mir = k >= a.fe;
-    m = mir ? a.brn - k : k;
-  } else {
-    mir = k >= a.fo;
-    m = mir ? a.brn - 1 - k : k;
-  }
-}
-
-template <typename C>
-struct ZParams {
-  C* B;
-  const C* ker;
-  const int* mapx;
-  const int* mapy;
-  const int* mapz;
-  const AxisPlan* pl;  // device copy
-  int P;
-  const C* tw;
-  int Px, Py;
-  int TX, ntiles;
-  int nin, nout;  // source / target z cells
-  int zb;         // z planes per channel in B
-  int tx, ty, tz; // stored kernel extents
-  int parT;
-  int nrhs;
-  double scale;
-  FDiv md;    // division by the tile width TX
-  FDiv nind;  // division by nin
-  AxMap ax[3];
-};
-
-// ky order that places each frequency next to its mirror Py - ky, and kx
-// tile order that places tile i next to tile ntiles-1-i, so that the four
-// CTAs reading the same stored (half-spectrum) kernel values run together and
-// the re-reads are served from L2.
-__device__ __forceinline__ int mirror_seq(int idx, int n) {
-  if (idx == 0) return 0;
-  if (n % 2 == 0) {
-    if (idx == 1) return n / 2;
-    const int k = (idx - 2) / 2 + 1;
-    return (idx % 2 == 0) ? k : n - k;
-  }
-  const int k = (idx - 1) / 2 + 1;
-  return (idx % 2 == 1) ? k : n - k;
-}
-__device__ __forceinline__ int tile_seq(int idx, int n) {
-  const int k = idx / 2;
-  return (idx % 2 == 0) ? k : n - 1 - k;
-}
-
-template <typename C>
-__device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c) {
-  return __ldg(g + c);
-}
-
-
-template <typename C, bool MX>
-__global__ void __launch_bounds__(512) k_z(const ZParams<C> p) {
-  using T = typename Real<C>::T;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const AxisPlan* const pl = p.pl;
-  const int P = p.P;
-  const int nrhs = p.nrhs, ntiles = p.ntiles, TX = p.TX, Px = p.Px, Py = p.Py;
-  const int nin = p.nin, nout = p.nout;
-  const int rhs = blockIdx.x % nrhs;
-  const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
-  const int kx0 = tile_seq(tseq, ntiles) * TX;
-  const int ky = mirror_seq(yseq, Py);
-  const int tmax = Px - kx0;
-  const int64_t plane = (int64_t)Py * Px;
-  const int CH = P * TX;  // one component's spectra in shared memory: [kz][t]
-  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
-  // stage all three components' source z lines into shared memory [c][z][t]
-  for (int q = threadIdx.x; q < 3 * nin * TX; q += blockDim.x) {
-    const int row = (int)p.md.div((uint32_t)q);  // c * nin + z
-    const int t = q - row * TX;
-    const int c = (int)p.nind.div((uint32_t)row);
-    const int i = row - c * nin;
-    if (t < tmax) cp_async(sm + c * CH + i * TX + t, Bb + (int64_t)row * plane + t);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  // forward, one component at a time, in place in shared memory
-  for (int c = 0; c < 3; ++c) {
-    C* const smc = sm + c * CH;
-    auto ldf = [=](int t, int i) -> C {
-      if (t < tmax && i < nin) return smc[i * TX + t];
-      return czero<C>();
-    };
-    auto lds = [=](int t, int i) -> C { return smc[i * TX + t]; };
-    auto sts = [=](int t, int i, C v) { smc[i * TX + t] = v; };
-    fft_run<C, StageE<MX>::v, false, true, MX>(pl, TX, p.md, p.tw, ldf, lds, sts, sts, true, true);
-  }
-
-  const int my = __ldg(p.mapy + ky);
-  const int py = (my >> 29) & 1, ry = (my >> 30) & 1;
-  const int iy = my & 0x1fffffff;
-  const int tx = p.tx, ty = p.ty, tz = p.tz, parT = p.parT;
-  const int* const mapx = p.mapx;
-  const int* const mapz = p.mapz;
-  const T s = (T)p.scale;
-  C* const out3 = sm + 3 * CH;  // extra 3-component buffer (parT > 1 only)
-  for (int t_par = 0; t_par < parT; ++t_par) {
-    C* const dst = (parT == 1) ? sm : out3;
-    const C* const kpar = p.ker + (int64_t)t_par * 8 * tz * ty * tx * 6;
-    for (int task = threadIdx.x; task < CH; task += blockDim.x) {
-      const int kz = (int)p.md.div((uint32_t)task);
-      const int t = task - kz * TX;
-      const int kx = kx0 + t;
-      if (kx >= Px) continue;
-      const int mx = __ldg(mapx + kx), mz = __ldg(mapz + kz);
-      const int px = (mx >> 29) & 1, rx = (mx >> 30) & 1, ix = mx & 0x1fffffff;
-      const int pz = (mz >> 29) & 1, rz = (mz >> 30) & 1, iz = mz & 0x1fffffff;
-      const int eo = 4 * px + 2 * py + pz;
-      const C* g = kpar + ((((int64_t)eo * tz + iz) * ty + iy) * tx + ix) * 6;
-      const T sxy = (rx ^ ry) ? (T)-1 : (T)1;
-      const T sxz = (rx ^ rz) ? (T)-1 : (T)1;
-      const T syz = (ry ^ rz) ? (T)-1 : (T)1;
-      const C gxx = ker_ld(g, 0), gyy = ker_ld(g, 1), gzz = ker_ld(g, 2);
-      const C gxy = cscale(ker_ld(g, 3), sxy), gxz = cscale(ker_ld(g, 4), sxz), gyz = cscale(ker_ld(g, 5), syz);
-      const C x0 = sm[task], x1 = sm[CH + task], x2 = sm[2 * CH + task];
-      C y0 = cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2));
-      C y1 = cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2));
-      C y2 = cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2));
-      dst[task] = cscale(y0, s);
-      dst[CH + task] = cscale(y1, s);
-      dst[2 * CH + task] = cscale(y2, s);
-    }
-    __syncthreads();
-    // inverse, one component at a time: shared -> global (target z), truncated
-    for (int c = 0; c < 3; ++c) {
-      C* const dc = dst + c * CH;
-      C* const Bo = Bb + (int64_t)(t_par * 3 + c) * nout * plane;
-      auto ldo = [=](int t, int i) -> C { return dc[i * TX + t]; };
-      auto sto = [=](int t, int i, C v) { dc[i * TX + t] = v; };
-      auto stg = [=](int t, int i, C v) {
-        if (t < tmax && i < nout) Bo[(int64_t)i * plane + t] = v;
-      };
-      fft_run<C, StageE<MX>::v, true, true, MX>(pl, TX, p.md, p.tw, ldo, ldo, sto, stg, true, false);
-    }
-  }
-}
-
-// -------------------------------------------------------------------- xinv
-template <typename C>
-struct XiParams {
-  const C* A;
-  C* out;
-  const AxisPlan* pl;  // device copy
-  int P;
-  const C* tw;
-  int nout;  // target x cells
-  int M;
-  int64_t rows;   // rows in this launch
-  int64_t g_off;  // global row index (over all rhs) of the first row
-  int ty, tz, parT;
-  int part_scatter;  // parT > 1
-  int tdiv[3];
-  int toff[64][3];
-  int64_t full[3];
-  C alpha, beta;
-  FDiv pd;  // division by P
-};
-
-template <typename C, bool AXPBY, bool MX>
-__global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const AxisPlan* const pl = p.pl;
-  const int P = p.P, M = p.M, nout = p.nout;
-  const int64_t rows = p.rows;
-  const C* const A = p.A;
-  C* const out = p.out;
-  const C alpha = p.alpha, beta = p.beta;
-  const int64_t g0 = (int64_t)blockIdx.x * M;
-  const bool scatter = p.part_scatter != 0;
-  const int ty = p.ty, tz = p.tz, parT = p.parT;
-  const int d0 = p.tdiv[0], d1 = p.tdiv[1], d2 = p.tdiv[2];
-  const int64_t f0 = p.full[0], f1 = p.full[1], f2 = p.full[2];
-  const int(*toff)[3] = p.toff;
-  const int64_t g_off = p.g_off;
-  const int LS = row_stride(P);
-  // stage the M spectral rows (P values each) into shared memory
-  {
-    const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
-    const C* const src = A + g0 * P;
-    for (int q = threadIdx.x; q < nl * P; q += blockDim.x) {
-      const int l = (int)p.pd.div((uint32_t)q);
-      const int i = q - l * P;
-      cp_async(sm + l * LS + i + (i >> 3), src + q);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  auto ldg = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
-  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
-  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
-  auto stg = [=](int l, int i, C v) {
-    const int64_t g = g0 + l;
-    if (g >= rows || i >= nout) return;
-    int64_t o;
-    const int64_t gg = g + g_off;
-    if (!scatter) {
-      o = gg * nout + i;
-    } else {
-      // gg = ((rhs*parT + t)*3 + c)*tz + z)*ty + y
-      int64_t q = gg;
-      const int y = (int)(q % ty); q /= ty;
-      const int z = (int)(q % tz); q /= tz;
-      const int c = (int)(q % 3); q /= 3;
-      const int t = (int)(q % parT);
-      const int64_t rhs = q / parT;
-      const int64_t X = (int64_t)i * d0 + toff[t][0];
-      const int64_t Y = (int64_t)y * d1 + toff[t][1];
-      const int64_t Z = (int64_t)z * d2 + toff[t][2];
-      o = (((rhs * 3 + c) * f2 + Z) * f1 + Y) * f0 + X;
-    }
-    if (AXPBY)
-      out[o] = cadd(cmul(alpha, v), cmul(beta, out[o]));
-    else
-      out[o] = v;
-  };
-  const FDiv md{1, 0, 0};
-  fft_run<C, StageE<MX>::v, true, false, MX>(pl, M, md, p.tw, ldg, lds, sts, stg, true, false);
-}
-
-// ------------------------------------------------ compile-time specialised
-// The same five passes with the transform length P, tile width and thread
-// count as template constants (see fft_ct.cuh).
-
-template <typename C, int P>
-__global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd_ct(const XfParams<C> p) {
-  constexpr int M = ct_xlines<sizeof(C)>(P);
-  constexpr int T = ct_threads(M, P);
-  constexpr int LS = P + (P + 7) / 8;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const int nin = p.nin;
-  const int64_t rows = p.rows;
-  C* const A = p.A;
-  const int64_t g0 = (int64_t)blockIdx.x * M;
-  {
-    const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
-    const C* const src = p.in + g0 * nin;
-    for (int q = threadIdx.x; q < nl * nin; q += T) {
-      const int l = (int)p.nind.div((uint32_t)q);
-      const int i = q - l * nin;
-      cp_async(sm + l * LS + i + (i >> 3), src + q);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  auto ldf = [=](int l, int i) -> C {
-    if (i < nin) return sm[l * LS + i + (i >> 3)];
-    return czero<C>();
-  };
-  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
-  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
-  auto stg = [=](int l, int i, C v) {
-    const int64_t g = g0 + l;
-    if (g < rows) A[g * P + i] = v;
-  };
-  ct_run<C, P, 8, T, M, false, false>(p.tw, ldf, lds, sts, stg, true, false);
-}
-
-template <typename C, int P, bool INV>
-__global__ void __launch_bounds__(ct_threads(ct_ytile<sizeof(C)>(P), P)) k_y_ct(const YParams<C> p) {
-  constexpr int TX = ct_ytile<sizeof(C)>(P);
-  constexpr int T = ct_threads(TX, P);
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const int Px = p.Px, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
-  const int64_t rc = slice / p.nz;
-  const int z = (int)(slice % p.nz);
-  const int kx0 = tile * TX;
-  const C* const src = p.src + ((rc * p.src_z + z) - p.src_sub) * p.src_rows * (int64_t)Px + kx0;
-  C* const dst = p.dst + ((rc * p.dst_z + z) - p.dst_sub) * p.dst_rows * (int64_t)Px + kx0;
-  const int tmax = Px - kx0;
-  for (int q = threadIdx.x; q < nin * TX; q += T) {
-    const int i = q / TX, t = q % TX;
-    if (t < tmax) cp_async(sm + q, src + (int64_t)i * Px + t);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-  auto ldf = [=](int t, int i) -> C {
-    if (t < tmax && i < nin) return sm[i * TX + t];
-    return czero<C>();
-  };
-  auto lds = [=](int t, int i) -> C { return sm[i * TX + t]; };
-  auto sts = [=](int t, int i, C v) { sm[i * TX + t] = v; };
-  auto stg = [=](int t, int i, C v) {
-    if (t < tmax && i < nout) dst[(int64_t)i * Px + t] = v;
-  };
-  ct_run<C, P, 8, T, TX, INV, true>(p.tw, ldf, lds, sts, stg, true, false);
-}
-
-template <typename C, int P>
-__global__ void __launch_bounds__(ct_threads(ct_ztile<sizeof(C)>(P), P)) k_z_ct(const ZParams<C> p) {
-  using Tr = typename Real<C>::T;
-  constexpr int TX = ct_ztile<sizeof(C)>(P);
-  constexpr int T = ct_threads(TX, P);
-  constexpr int CH = P * TX;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const int nrhs = p.nrhs, ntiles = p.ntiles, Px = p.Px, Py = p.Py;
-  const int nin = p.nin, nout = p.nout;
-  const int rhs = blockIdx.x % nrhs;
-  const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
-  const int kx0 = tile_seq(tseq, ntiles) * TX;
-  const int ky = mirror_seq(yseq, Py);
-  const int tmax = Px - kx0;
-  const int64_t plane = (int64_t)Py * Px;
-  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
-  for (int q = threadIdx.x; q < 3 * nin * TX; q += T) {
-    const int row = q / TX, t = q % TX;  // row = c * nin + z
-    const int c = (int)p.nind.div((uint32_t)row);
-    const int i = row - c * nin;
-    if (t < tmax) cp_async(sm + c * CH + i * TX + t, Bb + (int64_t)row * plane + t);
-  }
-  cp_async_wait_all();
-  __syncthreads();
-#pragma unroll 1
-  for (int c = 0; c < 3; ++c) {
-    C* const smc = sm + c * CH;
-    auto ldf = [=](int t, int i) -> C {
-      if (t < tmax && i < nin) return smc[i * TX + t];
-      return czero<C>();
-    };
-    auto lds = [=](int t, int i) -> C { return smc[i * TX + t]; };
-    auto sts = [=](int t, int i, C v) { smc[i * TX + t] = v; };
-    ct_run<C, P, 8, T, TX, false, true>(p.tw, ldf, lds, sts, sts, true, true);
-  }
-  int py, iy, ry;
-  ax_map(p.ax[1], ky, py, iy, ry);
-  const int tx = p.tx, ty = p.ty, tz = p.tz, parT = p.parT;
-  const Tr s = (Tr)p.scale;
-  C* const out3 = sm + 3 * CH;
-  // When the z axis is stored by symmetry, frequencies kz and P - kz read the
-  // same stored kernel value (mirrored: off-diagonal signs flip), so one task
-  // handles both.  Tasks: t = task % TX, kz = task / TX for kz <= P/2.
-  const bool zpair = !p.ax[2].full;
-  const int nzt = zpair ? (P / 2 + 1) : P;
-  for (int t_par = 0; t_par < parT; ++t_par) {
-    C* const dst = (parT == 1) ? sm : out3;
-    const C* const kpar = p.ker + (int64_t)t_par * 8 * tz * ty * tx * 6;
-    for (int task = threadIdx.x; task < nzt * TX; task += T) {
-      const int kz = task / TX, t = task % TX;
-      const int kx = kx0 + t;
-      if (kx >= Px) continue;
-      int px, ix, rx, pz, iz, rz;
-      ax_map(p.ax[0], kx, px, ix, rx);
-      ax_map(p.ax[2], kz, pz, iz, rz);
-      const int eo = 4 * px + 2 * py + pz;
-      const C* gp = kpar + ((((int64_t)eo * tz + iz) * ty + iy) * tx + ix) * 6;
-      const C gxx = ker_ld(gp, 0), gyy = ker_ld(gp, 1), gzz = ker_ld(gp, 2);
-      const C gxy = cscale(ker_ld(gp, 3), (rx ^ ry) ? (Tr)-1 : (Tr)1);
-      const C g4 = ker_ld(gp, 4), g5 = ker_ld(gp, 5);
-      // the task's own frequency, then (paired) its mirror with rz flipped
-      const int nk = (zpair && kz != 0 && 2 * kz != P) ? 2 : 1;
-#pragma unroll 1
-      for (int h = 0; h < nk; ++h) {
-        const int kk = h ? P - kz : kz;
-        const int rzz = h ? (rz ^ 1) : rz;
-        const C gxz = cscale(g4, (rx ^ rzz) ? (Tr)-1 : (Tr)1);
-        const C gyz = cscale(g5, (ry ^ rzz) ? (Tr)-1 : (Tr)1);
-        const int e = kk * TX + t;
-        const C x0 = sm[e], x1 = sm[CH + e], x2 = sm[2 * CH + e];
-        C y0 = cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2));
-        C y1 = cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2));
-        C y2 = cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2));
-        dst[e] = cscale(y0, s);
-        dst[CH + e] = cscale(y1, s);
-        dst[2 * CH + e] = cscale(y2, s);
-      }
-    }
-    __syncthreads();
-#pragma unroll 1
-    for (int c = 0; c < 3; ++c) {
-      C* const dc = dst + c * CH;
-      C* const Bo = Bb + (int64_t)(t_par * 3 + c) * nout * plane;
-      auto ldo = [=](int t, int i) -> C { return dc[i * TX + t]; };
-      auto sto = [=](int t, int i, C v) { dc[i * TX + t] = v; };
-      auto stg = [=](int t, int i, C v) {
-        if (t < tmax && i < nout) Bo[(int64_t)i * plane + t] = v;
-      };
-      ct_run<C, P, 8, T, TX, true, true>(p.tw, ldo, ldo, sto, stg, true, false);
-    }
-  }
-}
-
-template <typename C, int P, bool AXPBY>
-__global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv_ct(const XiParams<C> p) {
-  constexpr int M = ct_xlines<sizeof(C)>(P);
-  constexpr int T = ct_threads(M, P);
-  constexpr int LS = P + (P + 7) / 8;
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* const sm = reinterpret_cast<C*>(smem_raw);
-  const int nout = p.nout;
-  const int64_t rows = p.rows;
-  C* const out = p.out;
-  const C alpha = p.alpha, beta = p.beta;
-  const int64_t g0 = (int64_t)blockIdx.x * M;
-  const bool scatter = p.part_scatter != 0;
-  const int ty = p.ty, tz = p.tz, parT = p.parT;
-  const int d0 = p.tdiv[0], d1 = p.tdiv[1], d2 = p.tdiv[2];
-  const int64_t f0 = p.full[0], f1 = p.full[1], f2 = p.full[2];
-  const int(*toff)[3] = p.toff;
-  const int64_t g_off = p.g_off;
-  {
-    const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
-    const C* const src = p.A + g0 * P;
-    for (int q = threadIdx.x; q < nl * P; q += T) {
-      const int l = q / P, i = q % P;
-      cp_async(sm + l * LS + i + (i >> 3), src + q);
-    }
-    cp_async_wait_all();
-    __syncthreads();
-  }
-  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
-  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
-  auto stg = [=](int l, int i, C v) {
-    const int64_t g = g0 + l;
-    if (g >= rows || i >= nout) return;
-    int64_t o;
-    const int64_t gg = g + g_off;
-    if (!scatter) {
-      o = gg * nout + i;
-    } else {
-      int64_t q = gg;
-      const int y = (int)(q % ty); q /= ty;
-      const int z = (int)(q % tz); q /= tz;
-      const int c = (int)(q % 3); q /= 3;
-      const int t = (int)(q % parT);
-      const int64_t rhs = q / parT;
-      const int64_t X = (int64_t)i * d0 + toff[t][0];
-      const int64_t Y = (int64_t)y * d1 + toff[t][1];
-      const int64_t Z = (int64_t)z * d2 + toff[t][2];
-      o = (((rhs * 3 + c) * f2 + Z) * f1 + Y) * f0 + X;
-    }
-    if (AXPBY)
-      out[o] = cadd(cmul(alpha, v), cmul(beta, out[o]));
-    else
-      out[o] = v;
-  };
-  ct_run<C, P, 8, T, M, true, false>(p.tw, lds, lds, sts, stg, true, false);
-}
-
-// Lengths with specialised kernels.
-#define GILA_CT_SIZES(X) X(64) X(96) X(128) X(192) X(256) X(384) X(512)
-static bool ct_has(int P) {
-#define GILA_CT_CASE(n) if (P == n) return true;
-  GILA_CT_SIZES(GILA_CT_CASE)
-#undef GILA_CT_CASE
-  return false;
-}
-
-// ---------------------------------------------------------------- launchers
-static cudaError_t set_smem(const void* fn, size_t bytes) {
-  if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
-  return cudaSuccess;
-}
-
-static bool is_mixed(const AxisPlan& pl) {
-  for (int s = 0; s < pl.nst; ++s)
-    if (pl.radix[s] != 2 && pl.radix[s] != 4 && pl.radix[s] != 8) return true;
-  return false;
-}
-
 int pass_threads(const AxisPlan& pl, int M) {
-  const int E = is_mixed(pl) ? kEm : kE;
+  const int E = is_mixed_plan(pl) ? kEm : kE;
   int t = round_up((M * pl.P + E - 1) / E, 32);
   return t < 32 ? 32 : t;
-}
-
-#define GILA_LAUNCH(MXV, KERNEL, ...)                                                        \
-  do {                                                                                       \
-    const void* fn__ = (const void*)KERNEL;                                                  \
-    cudaError_t e__ = set_smem(fn__, sm);                                                    \
-    if (e__ != cudaSuccess) return e__;                                                      \
-    KERNEL<<<(unsigned)blocks, T, sm, st>>>(__VA_ARGS__);                                    \
-  } while (0)
-
-template <typename C>
-cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* A, int64_t rows,
-                        cudaStream_t st) {
-  XfParams<C> p;
-  p.in = in;
-  p.A = A;
-  p.pl = d.plan_d[0];
-  p.P = d.plan[0].P;
-  p.tw = d.tw[0];
-  p.nin = g.sc[0];
-  p.M = L.xf_lines;
-  p.rows = rows;
-  p.nind = make_fdiv((uint32_t)p.nin);
-  if (ct_has(p.P)) {
-#define GILA_CT_XF(n)                                                                  \
-  if (p.P == n) {                                                                      \
-    constexpr int M = ct_xlines<sizeof(C)>(n);                                         \
-    const int T = ct_threads(M, n);                                                    \
-    const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                           \
-    p.M = M;                                                                           \
-    const int64_t blocks = (p.rows + M - 1) / M;                                       \
-    GILA_LAUNCH(false, (k_xfwd_ct<C, n>), p);                                          \
-    return cudaGetLastError();                                                         \
-  }
-    GILA_CT_SIZES(GILA_CT_XF)
-#undef GILA_CT_XF
-  }
-  const int T = pass_threads(d.plan[0], p.M);
-  if (T > 512) return cudaErrorInvalidConfiguration;
-  const size_t sm = (size_t)p.M * row_stride(p.P) * sizeof(C);
-  const int64_t blocks = (p.rows + p.M - 1) / p.M;
-  if (is_mixed(d.plan[0]))
-    GILA_LAUNCH(true, (k_xfwd<C, true>), p);
-  else
-    GILA_LAUNCH(false, (k_xfwd<C, false>), p);
-  return cudaGetLastError();
-}
-
-template <typename C, bool INV>
-static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, cudaStream_t st) {
-  if (ct_has(p.P)) {
-#define GILA_CT_Y(n)                                  \
-  if (p.P == n) {                                     \
-    GILA_LAUNCH(false, (k_y_ct<C, n, INV>), p);       \
-    return cudaSuccess;                               \
-  }
-    GILA_CT_SIZES(GILA_CT_Y)
-#undef GILA_CT_Y
-  }
-  if (mx)
-    GILA_LAUNCH(true, (k_y<C, INV, true>), p);
-  else
-    GILA_LAUNCH(false, (k_y<C, INV, false>), p);
-  return cudaSuccess;
-}
-
-// One y pass over planes [q0, q0 + nq) (plane = ch*nz + z) of one rhs.
-// Forward: src = x-pass slab holding planes from src_sub on, dst = B of the
-// rhs.  Inverse: src = B of the rhs, dst = slab holding planes from dst_sub.
-template <typename C>
-cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int64_t q0,
-                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st) {
-  YParams<C> p;
-  p.src = src;
-  p.dst = dst;
-  p.pl = d.plan_d[1];
-  p.P = d.plan[1].P;
-  p.tw = d.tw[1];
-  p.Px = g.P[0];
-  p.TX = L.y_tx;
-  if (!inv) {
-    p.nin = g.sc[1];
-    p.nout = g.P[1];
-    p.nz = g.sc[2];
-    p.src_z = g.sc[2];
-    p.src_rows = g.sc[1];
-    p.dst_z = g.sc[2];  // B planes: c*sz + z
-    p.dst_rows = g.P[1];
-  } else {
-    p.nin = g.P[1];
-    p.nout = g.tc[1];
-    p.nz = g.tc[2];
-    p.src_z = g.tc[2];  // B planes: ch*tz + z
-    p.src_rows = g.P[1];
-    p.dst_z = g.tc[2];
-    p.dst_rows = g.tc[1];
-  }
-  p.q0 = q0;
-  p.src_sub = src_sub;
-  p.dst_sub = dst_sub;
-  if (ct_has(p.P)) {
-    int tx = 1;
-#define GILA_CT_YT(n) if (p.P == n) tx = ct_ytile<sizeof(C)>(n);
-    GILA_CT_SIZES(GILA_CT_YT)
-#undef GILA_CT_YT
-    p.TX = tx;
-  }
-  p.ntiles = (p.Px + p.TX - 1) / p.TX;
-  p.md = make_fdiv((uint32_t)p.TX);
-  const int T = ct_has(p.P) ? ct_threads(p.TX, p.P) : pass_threads(d.plan[1], p.TX);
-  if (T > 512) return cudaErrorInvalidConfiguration;
-  const size_t sm = (size_t)p.TX * p.P * sizeof(C);
-  const bool mx = is_mixed(d.plan[1]);
-  const int64_t blocks = (int64_t)p.ntiles * nq;
-  cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, st) : launch_y_one<C, false>(p, mx, T, sm, blocks, st);
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
-}
-
-template <typename C>
-cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st) {
-  const Work w = work_sizes(g);
-  ZParams<C> p;
-  p.B = B;
-  p.ker = d.ker;
-  p.mapx = d.map[0];
-  p.mapy = d.map[1];
-  p.mapz = d.map[2];
-  p.pl = d.plan_d[2];
-  p.P = d.plan[2].P;
-  p.tw = d.tw[2];
-  p.Px = g.P[0];
-  p.Py = g.P[1];
-  p.TX = L.z_tx;
-  p.nin = g.sc[2];
-  p.nout = g.tc[2];
-  p.zb = w.zb;
-  p.tx = g.tru[0];
-  p.ty = g.tru[1];
-  p.tz = g.tru[2];
-  p.parT = g.parT;
-  p.nrhs = nrhs;
-  p.scale = d.scale;
-  for (int k = 0; k < 3; ++k) {
-    p.ax[k].brn = g.P[k] / 2;
-    p.ax[k].full = g.tru[k] == g.P[k] / 2;
-    p.ax[k].fe = (g.tc[k] + 1) / 2 + (g.tc[k] % 2 == 0 ? 1 : 0);
-    p.ax[k].fo = (g.tc[k] + 1) / 2;
-  }
-  if (ct_has(p.P)) {
-    int tx = 1;
-#define GILA_CT_ZT(n) if (p.P == n) tx = ct_ztile<sizeof(C)>(n);
-    GILA_CT_SIZES(GILA_CT_ZT)
-#undef GILA_CT_ZT
-    p.TX = tx;
-  }
-  p.ntiles = (p.Px + p.TX - 1) / p.TX;
-  p.md = make_fdiv((uint32_t)p.TX);
-  p.nind = make_fdiv((uint32_t)p.nin);
-  const int T = ct_has(p.P) ? ct_threads(p.TX, p.P) : pass_threads(d.plan[2], p.TX);
-  if (T > 512) return cudaErrorInvalidConfiguration;
-  const size_t sm = (size_t)3 * p.TX * p.P * sizeof(C) * (g.parT > 1 ? 2 : 1);
-  const int64_t blocks = (int64_t)p.ntiles * p.Py * nrhs;
-  if (ct_has(p.P)) {
-#define GILA_CT_Z(n)                          \
-  if (p.P == n) {                             \
-    GILA_LAUNCH(false, (k_z_ct<C, n>), p);    \
-    return cudaGetLastError();                \
-  }
-    GILA_CT_SIZES(GILA_CT_Z)
-#undef GILA_CT_Z
-  }
-  if (is_mixed(d.plan[2]))
-    GILA_LAUNCH(true, (k_z<C, true>), p);
-  else
-    GILA_LAUNCH(false, (k_z<C, false>), p);
-  return cudaGetLastError();
-}
-
-template <typename C, bool AXPBY>
-static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, cudaStream_t st) {
-  if (ct_has(p.P)) {
-#define GILA_CT_XI(n)                                 \
-  if (p.P == n) {                                     \
-    GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY>), p);  \
-    return cudaSuccess;                               \
-  }
-    GILA_CT_SIZES(GILA_CT_XI)
-#undef GILA_CT_XI
-  }
-  if (mx)
-    GILA_LAUNCH(true, (k_xinv<C, AXPBY, true>), p);
-  else
-    GILA_LAUNCH(false, (k_xinv<C, AXPBY, false>), p);
-  return cudaSuccess;
-}
-
-// x inverse over `rows` spectral rows of the slab A; g_off is the global row
-// index (over all rhs) of the slab's first row, `out` the full output.
-template <typename C>
-cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int64_t rows,
-                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st) {
-  XiParams<C> p;
-  p.A = A;
-  p.out = out;
-  p.pl = d.plan_d[0];
-  p.P = d.plan[0].P;
-  p.tw = d.tw[0];
-  p.nout = g.tc[0];
-  p.M = L.xi_lines;
-  p.ty = g.tc[1];
-  p.tz = g.tc[2];
-  p.parT = g.parT;
-  p.rows = rows;
-  p.g_off = g_off;
-  p.part_scatter = g.parT > 1;
-  for (int k = 0; k < 3; ++k) {
-    p.tdiv[k] = g.tdiv[k];
-    p.full[k] = g.out_full[k];
-  }
-  for (int t = 0; t < g.parT && t < 64; ++t)
-    for (int k = 0; k < 3; ++k) p.toff[t][k] = g.toff[t][k];
-  p.alpha = alpha;
-  p.beta = beta;
-  p.pd = make_fdiv((uint32_t)p.P);
-  if (ct_has(p.P)) {
-    int m = 1;
-#define GILA_CT_XL(n) if (p.P == n) m = ct_xlines<sizeof(C)>(n);
-    GILA_CT_SIZES(GILA_CT_XL)
-#undef GILA_CT_XL
-    p.M = m;
-  }
-  const int T = ct_has(p.P) ? ct_threads(p.M, p.P) : pass_threads(d.plan[0], p.M);
-  if (T > 512) return cudaErrorInvalidConfiguration;
-  const size_t sm = (size_t)p.M * row_stride(p.P) * sizeof(C);
-  const bool mx = is_mixed(d.plan[0]);
-  const int64_t blocks = (p.rows + p.M - 1) / p.M;
-  cudaError_t e =
-      axpby ? launch_xinv_one<C, true>(p, mx, T, sm, blocks, st) : launch_xinv_one<C, false>(p, mx, T, sm, blocks, st);
-  if (e != cudaSuccess) return e;
-  return cudaGetLastError();
 }
 
 // The x and y passes run slab by slab over planes (ch, z) so that the slab
@@ -925,67 +79,29 @@ int64_t matvec_launches(const Geom& g, int nrhs) {
   return 2 * nf + 1 + 2 * ni;
 }
 
-template <typename C>
-cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out,
-                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st) {
-  cudaError_t e;
-  const Work w = work_sizes(g);
-  const int64_t nq_slab = w.slab_planes;
-  const int64_t in_rhs = (int64_t)3 * g.sc[0] * g.sc[1] * g.sc[2];
-  // planes (rhs, ch, z) are one flat index when B is dense across rhs
-  const int64_t fwd_planes = 3LL * g.sc[2];
-  const bool fwd_flat = (int64_t)w.zb == g.sc[2];
-  const int64_t inv_planes = 3LL * g.parT * g.tc[2];
-  const bool inv_flat = (int64_t)w.zb == (int64_t)g.parT * g.tc[2];
-  if (phase == 0) {
-    const int64_t nr = fwd_flat ? 1 : nrhs;
-    const int64_t span = fwd_flat ? fwd_planes * nrhs : fwd_planes;
-    for (int64_t r = 0; r < nr; ++r)
-      for (int64_t q0 = 0; q0 < span; q0 += nq_slab) {
-        const int64_t nq = (span - q0) < nq_slab ? (span - q0) : nq_slab;
-        const C* src = in + r * in_rhs + q0 * g.sc[1] * (int64_t)g.sc[0];
-        if ((e = launch_xfwd<C>(g, d, L, src, A, nq * g.sc[1], st)) != cudaSuccess) return e;
-        if ((e = launch_y<C>(g, d, L, false, A, B + r * w.b_rhs, q0, nq, q0, 0, st)) != cudaSuccess) return e;
-      }
-    return cudaSuccess;
-  }
-  if (phase == 1) return launch_z<C>(g, d, L, B, nrhs, st);
-  const int64_t nr = inv_flat ? 1 : nrhs;
-  const int64_t span = inv_flat ? inv_planes * nrhs : inv_planes;
-  for (int64_t r = 0; r < nr; ++r)
-    for (int64_t q0 = 0; q0 < span; q0 += nq_slab) {
-      const int64_t nq = (span - q0) < nq_slab ? (span - q0) : nq_slab;
-      if ((e = launch_y<C>(g, d, L, true, B + r * w.b_rhs, A, q0, nq, 0, q0, st)) != cudaSuccess) return e;
-      const int64_t g_off = (r * inv_planes + q0) * g.tc[1];
-      if ((e = launch_xinv<C>(g, d, L, A, out, nq * g.tc[1], g_off, axpby, alpha, beta, st)) != cudaSuccess)
-        return e;
-    }
-  return cudaSuccess;
+static bool ct_len(int P) {
+  for (int n : {64, 96, 128, 192, 256, 384, 512})
+    if (P == n) return true;
+  return false;
 }
 
-template <typename C>
-cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A, C* B,
-                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st) {
-  for (int ph = 0; ph < 3; ++ph) {
-    cudaError_t e = launch_matvec_phase<C>(ph, g, d, L, in, out, A, B, nrhs, axpby, alpha, beta, st);
-    if (e != cudaSuccess) return e;
-  }
-  return cudaSuccess;
+std::vector<int> ct_tiles(int cs, int P, bool z) {
+  std::vector<int> v;
+  if (!ct_len(P)) return v;
+  for (int tx : kTileSet)
+    if (z ? ct_z_ok(cs, P, tx) : ct_y_ok(cs, P, tx)) v.push_back(tx);
+  return v;
 }
 
-#define GILA_INST(C)                                                                                              \
-  template cudaError_t launch_matvec_phase<C>(int, const Geom&, const DevOp<C>&, const Launch&, const C*, C*, C*, \
-                                              C*, int, bool, C, C, cudaStream_t);                                 \
-  template cudaError_t launch_matvec<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, C*, C*, int,   \
-                                        bool, C, C, cudaStream_t);                                                \
-  template cudaError_t launch_xfwd<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
-                                      cudaStream_t);                                                              \
-  template cudaError_t launch_y<C>(const Geom&, const DevOp<C>&, const Launch&, bool, const C*, C*, int64_t,      \
-                                   int64_t, int64_t, int64_t, cudaStream_t);                                      \
-  template cudaError_t launch_z<C>(const Geom&, const DevOp<C>&, const Launch&, C*, int, cudaStream_t);           \
-  template cudaError_t launch_xinv<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
-                                      int64_t, bool, C, C, cudaStream_t);
-GILA_INST(double2)
-GILA_INST(float2)
+int ct_tile_pick(int cs, int P, int want, bool z) {
+  const std::vector<int> v = ct_tiles(cs, P, z);
+  for (int tx : v)
+    if (tx == want) return tx;
+  // default: the widest up to 128-byte rows
+  int best = v.empty() ? 1 : v.front();
+  for (int tx : v)
+    if (tx * cs <= 128) best = tx;
+  return best;
+}
 
 }  // namespace gila

@@ -1,6 +1,7 @@
 // matvec.cuh -- geometry of one Green-operator matvec and the launchers of its
 // five passes.  See matvec.cu for the kernels.
 #pragma once
+#include <vector>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -36,6 +37,15 @@ struct Work {
   int64_t b_rhs;        // elements of B per rhs
   int zb;               // z planes per component in B
 };
+
+// complex values staged per thread per FFT stage: power-of-two plans (radix
+// 2/4/8 only) and mixed plans (radix 3/5/7 too) are separate instantiations
+// so that the common case carries no register pressure from the odd radices.
+#ifndef GILA_KE_MIXED
+#define GILA_KE_MIXED 4
+#endif
+constexpr int kE = 8;
+constexpr int kEm = GILA_KE_MIXED;
 
 // Default slab size.  Slabs small enough to stay L2-resident between the x
 // and y passes cut HBM traffic but multiply the launch count; the default
@@ -92,5 +102,12 @@ cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, con
                                 C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st);
 // Threads per CTA of a pass over M lines of an axis plan.
 int pass_threads(const AxisPlan& pl, int M);
+
+// Tile widths (kx per CTA) of the compile-time specialised y (z = false) or
+// z (z = true) kernels for transform length P and complex size cs; empty when
+// P has no specialised kernels.  ct_tile_pick returns `want` when it is one
+// of them, else the default (128-byte rows, or the widest that fits).
+std::vector<int> ct_tiles(int cs, int P, bool z);
+int ct_tile_pick(int cs, int P, int want, bool z);
 
 }  // namespace gila

@@ -140,6 +140,13 @@ struct Server {
       gila_status s = init_core(ctx, &sh->vol, nullptr, &kopt, GILA_C128, g64);
       if (s == GILA_OK) s = build_kernel(*g64);
       if (s == GILA_OK && cfg.mixed) s = cast_core(ctx, *g64, GILA_C64, g32);
+      // launch shapes timed here, off the scheduler thread; the tuning
+      // workspaces are released (batches own theirs)
+      for (Core* c : {g64.get(), g32.get()})
+        if (s == GILA_OK && c) {
+          s = ensure_tuned(*c, 1);
+          release_work(*c);
+        }
       std::string err = s == GILA_OK ? "" : std::string(gila_last_error());
       {
         std::lock_guard<std::mutex> lk(mu);

@@ -1154,11 +1154,11 @@ gila_status make_ls_batch(Core& g64, Core* g32, int slots, const BatchCfg& cfg, 
   if (s != GILA_OK) return s;
   if (slots < 1 || slots > 65535) return fail(GILA_ERR_ARG, "slots must be in 1..65535");
   if (cfg.ell < 1 || cfg.ell > kMaxEll) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
+  // launch shapes of the operators (timed once per geometry, cached)
   for (Core* c : {&g64, g32}) {
-    if (c && !c->tuned) {
-      c->launch = default_launch(*c);
-      c->tuned = true;
-    }
+    if (!c || c->tuned) continue;
+    std::lock_guard<std::mutex> lk(c->mu);
+    if ((s = ensure_tuned(*c, 1)) != GILA_OK) return s;
   }
   if (cfg.mixed) {
     if (!g32) return fail(GILA_ERR_ARG, "the mixed solve needs the ComplexF32 operator");

@@ -159,6 +159,18 @@ gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes);
  * inverse FFT), ms[2] = inverse y/x passes, ms[3] = whole apply. */
 gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double ms[4]);
 
+/* Launch shapes.  tiles = {x-forward lines per CTA, x-inverse lines per CTA,
+ * y-pass kx tile, z-pass kx tile}.  No counterpart in the reference.  The
+ * first apply of an operator picks the y and z tiles by timing every compiled
+ * candidate on the operator's workspaces (cached per context and geometry;
+ * GILA_AUTOTUNE=0 keeps the defaults); gila_opr_autotune re-runs that for a
+ * batch of nrhs vectors; gila_opr_set_tiles forces tiles (entries <= 0 or
+ * not compiled for the transform length are ignored).  Tiles never change
+ * results, only speed. */
+gila_status gila_opr_autotune(gila_opr* opr, int64_t nrhs, int32_t tiles[4]);
+gila_status gila_opr_get_tiles(gila_opr* opr, int32_t tiles[4]);
+gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]);
+
 /* Number of kernels one apply of nrhs vectors launches. */
 gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n);
 
