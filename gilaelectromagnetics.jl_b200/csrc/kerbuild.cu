@@ -1059,11 +1059,11 @@ __global__ void k_extract(const Z* __restrict__ crc, int Px, int Py, int Pz, int
   const int64_t vol = (int64_t)Px * Py * Pz;
   const int64_t n = (int64_t)8 * tz * ty * tx * 6;
   for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x) {
-    int64_t q = o;
-    const int c = (int)(q % 6);
-    q /= 6;
+    int64_t q = o;  // o = (((eo * tz + iz) * ty + iy) * 6 + c) * tx + ix
     const int ix = (int)(q % tx);
     q /= tx;
+    const int c = (int)(q % 6);
+    q /= 6;
     const int iy = (int)(q % ty);
     q /= ty;
     const int iz = (int)(q % tz);

@@ -57,7 +57,7 @@ Work work_sizes(const Geom& g);
 // the device; Dev bundles the pointers for one dtype.
 template <typename C>
 struct DevOp {
-  const C* ker;      // [parT][8][tz][ty][tx][6]
+  const C* ker;      // [parT][8][tz][ty][6][tx]
   const int* map[3]; // per axis, per frequency f: m | p<<29 | mirrored<<30
   const C* tw[3];    // P-point twiddle tables
   AxisPlan plan[3];          // host copies (launch decisions)

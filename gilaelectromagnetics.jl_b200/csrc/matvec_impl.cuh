@@ -191,8 +191,17 @@ __device__ __forceinline__ int tile_seq(int idx, int n) {
 }
 
 template <typename C>
-__device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c) {
-  return __ldg(g + c);
+__device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c, int tx) {
+  return __ldg(g + (int64_t)c * tx);
+}
+// Stored kernel layout [parT][eo][tz][ty][6][tx]: for one stored (z, y) row
+// the six components are consecutive runs over x, so the threads of a warp
+// (consecutive kx of a tile) read consecutive entries of one component.
+// Returns the address of component 0 of entry (eo, iz, iy, ix).
+template <typename C>
+__device__ __forceinline__ const C* ker_at(const C* __restrict__ kpar, int eo, int iz, int iy, int ix, int tx, int ty,
+                                           int tz) {
+  return kpar + (((int64_t)eo * tz + iz) * ty + iy) * 6 * tx + ix;
 }
 
 
@@ -257,12 +266,13 @@ __global__ void __launch_bounds__(512) k_z(const ZParams<C> p) {
       const int px = (mx >> 29) & 1, rx = (mx >> 30) & 1, ix = mx & 0x1fffffff;
       const int pz = (mz >> 29) & 1, rz = (mz >> 30) & 1, iz = mz & 0x1fffffff;
       const int eo = 4 * px + 2 * py + pz;
-      const C* g = kpar + ((((int64_t)eo * tz + iz) * ty + iy) * tx + ix) * 6;
+      const C* g = ker_at(kpar, eo, iz, iy, ix, tx, ty, tz);
       const T sxy = (rx ^ ry) ? (T)-1 : (T)1;
       const T sxz = (rx ^ rz) ? (T)-1 : (T)1;
       const T syz = (ry ^ rz) ? (T)-1 : (T)1;
-      const C gxx = ker_ld(g, 0), gyy = ker_ld(g, 1), gzz = ker_ld(g, 2);
-      const C gxy = cscale(ker_ld(g, 3), sxy), gxz = cscale(ker_ld(g, 4), sxz), gyz = cscale(ker_ld(g, 5), syz);
+      const C gxx = ker_ld(g, 0, tx), gyy = ker_ld(g, 1, tx), gzz = ker_ld(g, 2, tx);
+      const C gxy = cscale(ker_ld(g, 3, tx), sxy), gxz = cscale(ker_ld(g, 4, tx), sxz),
+              gyz = cscale(ker_ld(g, 5, tx), syz);
       const C x0 = sm[task], x1 = sm[CH + task], x2 = sm[2 * CH + task];
       C y0 = cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2));
       C y1 = cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2));
@@ -511,9 +521,9 @@ __global__ void __launch_bounds__(ct_threads(TX, P)) k_z_ct(const ZParams<C> p) 
           ax_map(p.ax[0], kx0 + t, px, ix, rxv[j]);
           ax_map(p.ax[2], kz, pz, iz, rzv[j]);
           const int eo = 4 * px + 2 * py + pz;
-          const C* gp = kpar + ((((int64_t)eo * tz + iz) * ty + iy) * tx + ix) * 6;
+          const C* gp = ker_at(kpar, eo, iz, iy, ix, tx, ty, tz);
 #pragma unroll
-          for (int q = 0; q < 6; ++q) gv[j][q] = ker_ld(gp, q);
+          for (int q = 0; q < 6; ++q) gv[j][q] = ker_ld(gp, q, tx);
         }
       }
 #pragma unroll
@@ -646,17 +656,16 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
     // stored kernel (mirror / sign rules of mulBrnDev!)
     int px, ix, rx;
     ax_map(p.ax[0], kx0 + l, px, ix, rx);
-    const C* const kb = p.ker + (((int64_t)(4 * px + 2 * py) * tz) * ty + iy) * tx * 6 + (int64_t)ix * 6;
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
       const int kz = j + r * TPL;
       int pz, iz, rz;
       ax_map(p.ax[2], kz, pz, iz, rz);
-      const C* gp = kb + ((int64_t)pz * tz + iz) * ty * tx * 6;
-      const C gxx = ker_ld(gp, 0), gyy = ker_ld(gp, 1), gzz = ker_ld(gp, 2);
-      const C gxy = cscale(ker_ld(gp, 3), (rx ^ ry) ? (Tr)-1 : (Tr)1);
-      const C gxz = cscale(ker_ld(gp, 4), (rx ^ rz) ? (Tr)-1 : (Tr)1);
-      const C gyz = cscale(ker_ld(gp, 5), (ry ^ rz) ? (Tr)-1 : (Tr)1);
+      const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
+      const C gxx = ker_ld(gp, 0, tx), gyy = ker_ld(gp, 1, tx), gzz = ker_ld(gp, 2, tx);
+      const C gxy = cscale(ker_ld(gp, 3, tx), (rx ^ ry) ? (Tr)-1 : (Tr)1);
+      const C gxz = cscale(ker_ld(gp, 4, tx), (rx ^ rz) ? (Tr)-1 : (Tr)1);
+      const C gyz = cscale(ker_ld(gp, 5, tx), (ry ^ rz) ? (Tr)-1 : (Tr)1);
       const C x0 = v[0][r], x1 = v[1][r], x2 = v[2][r];
       v[0][r] = cscale(cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2)), s);
       v[1][r] = cscale(cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2)), s);
