@@ -61,6 +61,29 @@ __device__ __forceinline__ C twid(const C* __restrict__ tw, int m) {
   return INV ? cconj(w) : w;
 }
 
+// Twiddles w^(r*step), r = 1 .. R-1, of one butterfly into w[1..R).  FP64:
+// w^step (and w^(4 step) for R = 8) from the table, the other powers by
+// complex products (a few FP64 multiplies instead of table loads, which
+// share the load/store pipe with the shared-memory transposes; the products
+// add at most 3 roundings).  FP32: table loads (its pipes are issue-bound).
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void twiddles(const C* __restrict__ tw, int step, C* w) {
+  if constexpr (sizeof(C) == 16 && (R == 4 || R == 8)) {
+    w[1] = twid<INV>(tw, step);
+    w[2] = cmul(w[1], w[1]);
+    w[3] = cmul(w[2], w[1]);
+    if constexpr (R == 8) {
+      w[4] = twid<INV>(tw, 4 * step);
+      w[5] = cmul(w[4], w[1]);
+      w[6] = cmul(w[4], w[2]);
+      w[7] = cmul(w[4], w[3]);
+    }
+  } else {
+#pragma unroll
+    for (int r = 1; r < R; ++r) w[r] = twid<INV>(tw, r * step);
+  }
+}
+
 // ------------------------------------------------------------- butterflies
 // In-place R-point DFT of v[0..R): out[k] = sum_r v[r] exp(-+2 pi i r k / R)
 // (minus sign forward, plus sign inverse), natural output order.
@@ -174,6 +197,10 @@ __device__ __forceinline__ void cp_async(double2* s, const double2* g) {
 __device__ __forceinline__ void cp_async(float2* s, const float2* g) {
   const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(g) : "memory");
+}
+__device__ __forceinline__ void cp_async(float4* s, const float4* g) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(s);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(sa), "l"(g) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 

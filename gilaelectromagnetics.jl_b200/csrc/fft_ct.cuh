@@ -114,9 +114,10 @@ __device__ __forceinline__ void ct_stage(const C* __restrict__ tw, const Ld& ld,
       }
       const int jm = j % NS;
       if (NS > 1) {
-        const int step = jm * TWST;
+        C w[R];
+        twiddles<R, INV>(tw, jm * TWST, w);
 #pragma unroll
-        for (int r = 1; r < R; ++r) v[k][r] = cmul(v[k][r], twid<INV>(tw, r * step));
+        for (int r = 1; r < R; ++r) v[k][r] = cmul(v[k][r], w[r]);
       }
       Bfly<R, INV, C>::run(v[k], tw, TPL);
       const int base = (j - jm) * R + jm;
@@ -157,6 +158,81 @@ __device__ __forceinline__ void ct_run(const C* __restrict__ tw, const LdF& ld_f
                                                                       first_in_smem, last_in_smem);
 }
 
+// ---------------------------------------------------------- line pairs
+// FP32 passes whose lines are contiguous in shared memory ([index][line]):
+// a task handles two adjacent lines, so each shared-memory access moves both
+// lines' values in one 16-byte transaction and the two lines share the
+// twiddles and the index arithmetic.  M2 = line pairs; ld / st take a pair
+// index and a position and move float4 = (line 2p, line 2p + 1).
+template <int P, int S, int T, int M2, bool INV, bool REV, class Ld, class St>
+__device__ __forceinline__ void ct_stage2(const float2* __restrict__ tw, const Ld& ld, const St& st, bool sync_mid) {
+  constexpr int R = ct_radix_o<REV>(P, S);
+  constexpr int NS = ct_span_o<REV>(P, S);
+  constexpr int TPL = P / R;
+  constexpr int NTASK = M2 * TPL;
+  constexpr int K = (NTASK + T - 1) / T;
+  constexpr int TWST = P / (NS * R);
+  float2 a[K][R], b[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NTASK % T == 0 || task < NTASK) {
+      const int lp = task % M2, j = task / M2;
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const float4 q = ld(lp, j + r * TPL);
+        a[k][r] = make_float2(q.x, q.y);
+        b[k][r] = make_float2(q.z, q.w);
+      }
+    }
+  }
+  if (sync_mid) __syncthreads();
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NTASK % T == 0 || task < NTASK) {
+      const int lp = task % M2, j = task / M2;
+      const int jm = j % NS;
+      if (NS > 1) {
+        float2 w[R];
+        twiddles<R, INV>(tw, jm * TWST, w);
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          a[k][r] = cmul(a[k][r], w[r]);
+          b[k][r] = cmul(b[k][r], w[r]);
+        }
+      }
+      Bfly<R, INV, float2>::run(a[k], tw, TPL);
+      Bfly<R, INV, float2>::run(b[k], tw, TPL);
+      const int base = (j - jm) * R + jm;
+#pragma unroll
+      for (int r = 0; r < R; ++r)
+        st(lp, base + r * NS, make_float4(a[k][r].x, a[k][r].y, b[k][r].x, b[k][r].y));
+    }
+  }
+}
+
+template <int P, int S0, int S, int S1, int T, int M2, bool INV, bool REV, class LdF, class LdM, class StM, class StL>
+__device__ __forceinline__ void ct_run_range2(const float2* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
+                                              const StM& st_mid, const StL& st_last, bool first_in_smem,
+                                              bool last_in_smem) {
+  if constexpr (S < S1) {
+    constexpr bool first = (S == S0), last = (S == S1 - 1);
+    const bool sync_mid = (first ? first_in_smem : true) && (last ? last_in_smem : true);
+    if constexpr (first && last)
+      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_first, st_last, sync_mid);
+    else if constexpr (first)
+      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_first, st_mid, sync_mid);
+    else if constexpr (last)
+      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_mid, st_last, sync_mid);
+    else
+      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_mid, st_mid, sync_mid);
+    __syncthreads();
+    ct_run_range2<P, S0, S + 1, S1, T, M2, INV, REV>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem,
+                                                     last_in_smem);
+  }
+}
+
 // ---------------------------------------------------------- launch shapes
 // Shared by the kernels (template constants) and the host (launch config).
 constexpr int ct_round32(int a) { return (a + 31) / 32 * 32; }
@@ -183,6 +259,8 @@ constexpr int ct_threads(int M, int P) {
   int t = ct_round32((M * P + 7) / 8);
   return t < 32 ? 32 : t;
 }
+// threads of a line-pair kernel over M lines (8 pairs of values per thread)
+constexpr int ct_threads2(int M, int P) { return ct_threads(M / 2, P); }
 // tile widths the y and z kernels are instantiated for (the autotuner picks
 // among them per operator): at most 512 threads and the shared-memory budget
 constexpr int kTileSet[3] = {4, 8, 16};

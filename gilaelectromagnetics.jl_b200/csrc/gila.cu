@@ -329,6 +329,9 @@ gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* sr
         g.toff[t][2] = z;
       }
   tru_inf(*core, g.tru);
+  // the z pass addresses one partition's kernel with 32-bit offsets
+  if ((int64_t)48 * g.tru[0] * g.tru[1] * g.tru[2] >= ((int64_t)1 << 31))
+    return fail(GILA_ERR_SIZE, "Fourier kernel too large: more than 2^31 stored values per target partition");
   for (int k = 0; k < 3; ++k) {
     if ((s = plan_axis(g.P[k], &core->plan[k])) != GILA_OK) return s;
     if ((s = twiddle_table(ctx->impl, g.P[k], dtype, &core->tw[k])) != GILA_OK) return s;

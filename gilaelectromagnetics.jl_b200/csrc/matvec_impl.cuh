@@ -192,7 +192,7 @@ __device__ __forceinline__ int tile_seq(int idx, int n) {
 
 template <typename C>
 __device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c, int tx) {
-  return __ldg(g + (int64_t)c * tx);
+  return __ldg(g + c * tx);
 }
 // Stored kernel layout [parT][eo][tz][ty][6][tx]: for one stored (z, y) row
 // the six components are consecutive runs over x, so the threads of a warp
@@ -201,7 +201,8 @@ __device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c, int tx) {
 template <typename C>
 __device__ __forceinline__ const C* ker_at(const C* __restrict__ kpar, int eo, int iz, int iy, int ix, int tx, int ty,
                                            int tz) {
-  return kpar + (((int64_t)eo * tz + iz) * ty + iy) * 6 * tx + ix;
+  // one partition holds 8 * tz * ty * 6 * tx < 2^31 entries (host-checked)
+  return kpar + ((((eo * tz + iz) * ty + iy) * 6) * tx + ix);
 }
 
 
@@ -645,12 +646,15 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
 #pragma unroll
       for (int r = 0; r < RL; ++r) v[c][r] = sm[c * CH + (j + r * TPL) * TX + l];
     // forward last stage (span TPL: twiddle exponent r * j)
+    {
+      C w[RL];
+      twiddles<RL, false>(tw, j, w);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      if (NST > 1)
+      for (int c = 0; c < 3; ++c) {
 #pragma unroll
-        for (int r = 1; r < RL; ++r) v[c][r] = cmul(v[c][r], twid<false>(tw, r * j));
-      Bfly<RL, false, C>::run(v[c], tw, TPL);
+        for (int r = 1; r < RL; ++r) v[c][r] = cmul(v[c][r], w[r]);
+        Bfly<RL, false, C>::run(v[c], tw, TPL);
+      }
     }
     // v[c][r] is frequency kz = j + r * TPL: 3x3 symmetric multiply with the
     // stored kernel (mirror / sign rules of mulBrnDev!)
@@ -695,6 +699,143 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
       if (t < tmax && i < nout) Bo[(int64_t)i * plane + t] = v;
     };
     ct_run_range<C, P, 1, 1, NST, 8, T, TX, true, true, true>(p.tw, ldp, ldo, sto, stg, true, false);
+  }
+}
+
+// The fused z pass for FP32 on line pairs (ct_stage2): same arithmetic as
+// k_zf_ct, each task moving two adjacent kx lines per shared-memory access.
+#ifndef GILA_ZF2_CAP
+#define GILA_ZF2_CAP 1
+#endif
+template <int P, int TX>
+__global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf_min_blocks(ct_threads2(TX, P)) : 1)
+    k_zf2_ct(const ZParams<float2> p) {
+  using C = float2;
+  constexpr int T = ct_threads2(TX, P);
+  constexpr int M2 = TX / 2;
+  constexpr int CH = P * TX;
+  constexpr int NST = ct_nst(P);
+  constexpr int RL = ct_radix(P, NST - 1);
+  constexpr int TPL = P / RL;
+  constexpr int NTASK = M2 * TPL;
+  constexpr int K = (NTASK + T - 1) / T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nrhs = p.nrhs, ntiles = p.ntiles, Px = p.Px, Py = p.Py;
+  const int nin = p.nin, nout = p.nout;
+  const int rhs = blockIdx.x % nrhs;
+  const int rest = blockIdx.x / nrhs;
+  const int tseq = rest % ntiles;
+  const int yseq = rest / ntiles;
+  const int kx0 = tile_seq(tseq, ntiles) * TX;
+  const int ky = mirror_seq(yseq, Py);
+  const int tmax = Px - kx0;  // even: Px and kx0 are even
+  const int64_t plane = (int64_t)Py * Px;
+  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
+  // stage the tile with 16-byte copies (pairs of columns)
+  for (int q = threadIdx.x; q < 3 * nin * M2; q += T) {
+    const int row = q / M2, t2 = q % M2;  // row = c * nin + z
+    const int c = (int)p.nind.div((uint32_t)row);
+    const int i = row - c * nin;
+    if (2 * t2 < tmax) cp_async(reinterpret_cast<float4*>(sm + c * CH + i * TX) + t2,
+                                reinterpret_cast<const float4*>(Bb + (int64_t)row * plane) + t2);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    float4* const smc = reinterpret_cast<float4*>(sm + c * CH);
+    auto ldf = [=](int t2, int i) -> float4 {
+      if (2 * t2 < tmax && i < nin) return smc[i * M2 + t2];
+      return z4;
+    };
+    auto lds = [=](int t2, int i) -> float4 { return smc[i * M2 + t2]; };
+    auto sts = [=](int t2, int i, float4 v) { smc[i * M2 + t2] = v; };
+    ct_run_range2<P, 0, 0, NST - 1, T, M2, false, false>(p.tw, ldf, lds, sts, sts, true, true);
+  }
+  int py, iy, ry;
+  ax_map(p.ax[1], ky, py, iy, ry);
+  const int tx = p.tx, ty = p.ty, tz = p.tz;
+  const float s = (float)p.scale;
+  const C* const tw = p.tw;
+  const float4* const sm4 = reinterpret_cast<const float4*>(sm);
+  float4* const smw = reinterpret_cast<float4*>(sm);
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NTASK % T != 0 && task >= NTASK) continue;
+    const int lp = task % M2, j = task / M2;
+    if (2 * lp >= tmax) continue;
+    C a[3][RL], b[3][RL];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const float4 q = sm4[(c * CH + (j + r * TPL) * TX) / 2 + lp];
+        a[c][r] = make_float2(q.x, q.y);
+        b[c][r] = make_float2(q.z, q.w);
+      }
+    {
+      C w[RL];
+      twiddles<RL, false>(tw, j, w);
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+#pragma unroll
+        for (int r = 1; r < RL; ++r) {
+          a[c][r] = cmul(a[c][r], w[r]);
+          b[c][r] = cmul(b[c][r], w[r]);
+        }
+        Bfly<RL, false, C>::run(a[c], tw, TPL);
+        Bfly<RL, false, C>::run(b[c], tw, TPL);
+      }
+    }
+    // the two columns kx0 + 2 lp (even parity) and kx0 + 2 lp + 1 (odd)
+    int pxa, ixa, rxa, pxb, ixb, rxb;
+    ax_map(p.ax[0], kx0 + 2 * lp, pxa, ixa, rxa);
+    ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+#pragma unroll
+    for (int r = 0; r < RL; ++r) {
+      const int kz = j + r * TPL;
+      int pz, iz, rz;
+      ax_map(p.ax[2], kz, pz, iz, rz);
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int px = h ? pxb : pxa, ix = h ? ixb : ixa, rx = h ? rxb : rxa;
+        const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
+        const C gxx = ker_ld(gp, 0, tx), gyy = ker_ld(gp, 1, tx), gzz = ker_ld(gp, 2, tx);
+        const C gxy = cscale(ker_ld(gp, 3, tx), (rx ^ ry) ? -1.f : 1.f);
+        const C gxz = cscale(ker_ld(gp, 4, tx), (rx ^ rz) ? -1.f : 1.f);
+        const C gyz = cscale(ker_ld(gp, 5, tx), (ry ^ rz) ? -1.f : 1.f);
+        C (*v)[RL] = h ? b : a;
+        const C x0 = v[0][r], x1 = v[1][r], x2 = v[2][r];
+        v[0][r] = cscale(cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2)), s);
+        v[1][r] = cscale(cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2)), s);
+        v[2][r] = cscale(cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2)), s);
+      }
+    }
+    // inverse first stage, written back to the slots the task read
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Bfly<RL, true, C>::run(a[c], tw, TPL);
+      Bfly<RL, true, C>::run(b[c], tw, TPL);
+#pragma unroll
+      for (int r = 0; r < RL; ++r)
+        smw[(c * CH + (j + r * TPL) * TX) / 2 + lp] = make_float4(a[c][r].x, a[c][r].y, b[c][r].x, b[c][r].y);
+    }
+  }
+  __syncthreads();
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    float4* const dc = reinterpret_cast<float4*>(sm + c * CH);
+    C* const Bo = Bb + (int64_t)c * nout * plane;
+    auto ldp = [=](int t2, int q) -> float4 { return dc[((q / RL) + (q % RL) * TPL) * M2 + t2]; };
+    auto ldo = [=](int t2, int i) -> float4 { return dc[i * M2 + t2]; };
+    auto sto = [=](int t2, int i, float4 v) { dc[i * M2 + t2] = v; };
+    auto stg = [=](int t2, int i, float4 v) {
+      if (2 * t2 < tmax && i < nout) reinterpret_cast<float4*>(Bo + (int64_t)i * plane)[t2] = v;
+    };
+    ct_run_range2<P, 1, 1, NST, T, M2, true, true>(p.tw, ldp, ldo, sto, stg, true, false);
   }
 }
 
@@ -765,13 +906,25 @@ static bool ct_has(int P) {
 }
 
 // ---------------------------------------------------------------- launchers
-// fused z pass (GILA_ZFUSE=0 selects the unfused one)
+// fused z pass (GILA_ZFUSE=0 selects the unfused one); FP32 on line pairs
+// (GILA_ZPAIR=0 selects one line per task)
 static inline bool zfuse() {
   static const bool on = [] {
     const char* e = getenv("GILA_ZFUSE");
     return !(e && e[0] == '0');
   }();
   return on;
+}
+static inline bool zpair() {
+  static const bool on = [] {
+    const char* e = getenv("GILA_ZPAIR");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+template <typename C>
+static inline const ZParams<float2>& zp32(const ZParams<C>& p) {
+  return reinterpret_cast<const ZParams<float2>&>(p);
 }
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
@@ -945,6 +1098,16 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
     if (p.P == n && p.TX == tx) {                     \
       if constexpr (zf_ok(sizeof(C), n)) {            \
         if (p.parT == 1 && zfuse()) {                 \
+          if constexpr (sizeof(C) == 8) {             \
+            if (zpair()) {                            \
+              const int T2 = ct_threads2(tx, n);      \
+              const void* fn2 = (const void*)k_zf2_ct<n, tx>; \
+              cudaError_t e2 = set_smem(fn2, sm);     \
+              if (e2 != cudaSuccess) return e2;       \
+              k_zf2_ct<n, tx><<<(unsigned)blocks, T2, sm, st>>>(zp32(p)); \
+              return cudaGetLastError();              \
+            }                                         \
+          }                                           \
           GILA_LAUNCH(false, (k_zf_ct<C, n, tx>), p); \
           return cudaGetLastError();                  \
         }                                             \
