@@ -451,6 +451,41 @@ __global__ void __launch_bounds__(ct_threads(TX, P)) k_y_ct(const YParams<C> p) 
   ct_run<C, P, 8, T, TX, INV, true>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
+// FP32 y pass on line pairs (ct_stage2): two adjacent kx columns per task.
+template <int P, bool INV, int TX>
+__global__ void __launch_bounds__(ct_threads2(TX, P)) k_y2_ct(const YParams<float2> p) {
+  constexpr int T = ct_threads2(TX, P);
+  constexpr int M2 = TX / 2;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int Px = p.Px, nin = p.nin, nout = p.nout;
+  const int tile = blockIdx.x % p.ntiles;
+  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int64_t rc = slice / p.nz;
+  const int z = (int)(slice % p.nz);
+  const int kx0 = tile * TX;
+  const float2* const src = p.src + ((rc * p.src_z + z) - p.src_sub) * p.src_rows * (int64_t)Px + kx0;
+  float2* const dst = p.dst + ((rc * p.dst_z + z) - p.dst_sub) * p.dst_rows * (int64_t)Px + kx0;
+  const int tmax = Px - kx0;  // even: Px and kx0 are even
+  for (int q = threadIdx.x; q < nin * M2; q += T) {
+    const int i = q / M2, t2 = q % M2;
+    if (2 * t2 < tmax) cp_async(sm + q, reinterpret_cast<const float4*>(src + (int64_t)i * Px) + t2);
+  }
+  cp_async_wait_all();
+  __syncthreads();
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto ldf = [=](int t2, int i) -> float4 {
+    if (2 * t2 < tmax && i < nin) return sm[i * M2 + t2];
+    return z4;
+  };
+  auto lds = [=](int t2, int i) -> float4 { return sm[i * M2 + t2]; };
+  auto sts = [=](int t2, int i, float4 v) { sm[i * M2 + t2] = v; };
+  auto stg = [=](int t2, int i, float4 v) {
+    if (2 * t2 < tmax && i < nout) reinterpret_cast<float4*>(dst + (int64_t)i * Px)[t2] = v;
+  };
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, INV, false>(p.tw, ldf, lds, sts, stg, true, false);
+}
+
 template <typename C, int P, int TX>
 __global__ void __launch_bounds__(ct_threads(TX, P)) k_z_ct(const ZParams<C> p) {
   using Tr = typename Real<C>::T;
@@ -926,6 +961,10 @@ template <typename C>
 static inline const ZParams<float2>& zp32(const ZParams<C>& p) {
   return reinterpret_cast<const ZParams<float2>&>(p);
 }
+template <typename C>
+static inline const YParams<float2>& yp32(const YParams<C>& p) {
+  return reinterpret_cast<const YParams<float2>&>(p);
+}
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
   if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -990,6 +1029,16 @@ static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, 
 #define GILA_CT_Y2(n, tx)                                  \
   if constexpr (ct_y_ok(sizeof(C), n, tx)) {               \
     if (p.P == n && p.TX == tx) {                          \
+      if constexpr (sizeof(C) == 8) {                      \
+        if (zpair()) {                                     \
+          const int T2 = ct_threads2(tx, n);               \
+          const void* fn2 = (const void*)k_y2_ct<n, INV, tx>; \
+          cudaError_t e2 = set_smem(fn2, sm);              \
+          if (e2 != cudaSuccess) return e2;                \
+          k_y2_ct<n, INV, tx><<<(unsigned)blocks, T2, sm, st>>>(yp32(p)); \
+          return cudaSuccess;                              \
+        }                                                  \
+      }                                                    \
       GILA_LAUNCH(false, (k_y_ct<C, n, INV, tx>), p);      \
       return cudaSuccess;                                  \
     }                                                      \
