@@ -477,6 +477,11 @@ static std::string tune_key(const Core& c, int64_t nrhs) {
   return b;
 }
 
+static bool tune_debug() {
+  const char* e = getenv("GILA_TUNE_DEBUG");
+  return e && e[0] == '1';
+}
+
 template <typename C>
 static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
@@ -526,6 +531,7 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
       L.z_tx = tx;
       const float t = time_of(L, {1});
       if (e != cudaSuccess) break;
+      if (tune_debug()) fprintf(stderr, "gila autotune dtype %d z tile %d: %.4f ms\n", (int)c.dtype, tx, t);
       if (t < bt) {
         bt = t;
         pick = tx;
@@ -541,6 +547,7 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
       L.y_tx = tx;
       const float t = time_of(L, {0, 2});
       if (e != cudaSuccess) break;
+      if (tune_debug()) fprintf(stderr, "gila autotune dtype %d y tile %d: %.4f ms\n", (int)c.dtype, tx, t);
       if (t < bt) {
         bt = t;
         pick = tx;

@@ -73,9 +73,19 @@ struct Launch {
   int z_tx;      // kx tile, z pass
 };
 
+// Lippmann-Schwinger epilogue of the last pass (self operators): out =
+// in - chi .* (G in), chi per cell broadcast over the three components,
+// chi_rs = 0 (one medium) or V (one per right-hand side of the launch).
+template <typename C>
+struct LsEpi {
+  const C* in;
+  const C* chi;
+  int64_t chi_rs;
+};
+
 template <typename C>
 cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A, C* B,
-                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st);
+                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls = nullptr);
 
 // Individual passes (exposed for the autotuner and the profiler).
 template <typename C>
@@ -88,7 +98,7 @@ template <typename C>
 cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st);
 template <typename C>
 cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int64_t rows,
-                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st);
+                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls = nullptr);
 
 int smem_optin_bytes();
 
@@ -99,7 +109,8 @@ int64_t matvec_launches(const Geom& g, int nrhs);
 // inverse y/x slabs.
 template <typename C>
 cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out,
-                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st);
+                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st,
+                                const LsEpi<C>* ls = nullptr);
 // Threads per CTA of a pass over M lines of an axis plan.
 int pass_threads(const AxisPlan& pl, int M);
 

@@ -316,7 +316,25 @@ struct XiParams {
   int64_t full[3];
   C alpha, beta;
   FDiv pd;  // division by P
+  // Lippmann-Schwinger epilogue (ls != 0): out = ls_in - chi .* value
+  const C* ls_in;
+  const C* ls_chi;
+  int64_t ls_chi_rs;
+  int ls;
+  FDiv rows_rhs;  // division by 3 * tz * ty (rows per right-hand side)
+  FDiv rows_zy;   // division by tz * ty
 };
+
+// the epilogue value at output index o of row gg, column i
+template <typename C>
+__device__ __forceinline__ C ls_value(const C* __restrict__ in, const C* __restrict__ chi, int64_t chi_rs, FDiv rr,
+                                      FDiv rzy, int nout, int64_t gg, int i, int64_t o, C v) {
+  const uint32_t rhs = rr.div((uint32_t)gg);
+  const uint32_t rem = (uint32_t)gg - rhs * rr.d;
+  const uint32_t zy = rem - rzy.div(rem) * rzy.d;
+  const C c = chi[(int64_t)rhs * chi_rs + (int64_t)zy * nout + i];
+  return csub(in[o], cmul(c, v));
+}
 
 template <typename C, bool AXPBY, bool MX>
 __global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
@@ -328,6 +346,11 @@ __global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
   const C* const A = p.A;
   C* const out = p.out;
   const C alpha = p.alpha, beta = p.beta;
+  const int ls = p.ls;
+  const C* const ls_in = p.ls_in;
+  const C* const ls_chi = p.ls_chi;
+  const int64_t ls_chi_rs = p.ls_chi_rs;
+  const FDiv rows_rhs = p.rows_rhs, rows_zy = p.rows_zy;
   const int64_t g0 = (int64_t)blockIdx.x * M;
   const bool scatter = p.part_scatter != 0;
   const int ty = p.ty, tz = p.tz, parT = p.parT;
@@ -373,6 +396,8 @@ __global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
     }
     if (AXPBY)
       out[o] = cadd(cmul(alpha, v), cmul(beta, out[o]));
+    else if (ls)
+      out[o] = ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, v);
     else
       out[o] = v;
   };
@@ -885,6 +910,11 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv
   const int64_t rows = p.rows;
   C* const out = p.out;
   const C alpha = p.alpha, beta = p.beta;
+  const int ls = p.ls;
+  const C* const ls_in = p.ls_in;
+  const C* const ls_chi = p.ls_chi;
+  const int64_t ls_chi_rs = p.ls_chi_rs;
+  const FDiv rows_rhs = p.rows_rhs, rows_zy = p.rows_zy;
   const int64_t g0 = (int64_t)blockIdx.x * M;
   const bool scatter = p.part_scatter != 0;
   const int ty = p.ty, tz = p.tz, parT = p.parT;
@@ -925,6 +955,8 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv
     }
     if (AXPBY)
       out[o] = cadd(cmul(alpha, v), cmul(beta, out[o]));
+    else if (ls)
+      out[o] = ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, v);
     else
       out[o] = v;
   };
@@ -1200,8 +1232,15 @@ static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t 
 // index (over all rhs) of the slab's first row, `out` the full output.
 template <typename C>
 cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int64_t rows,
-                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st) {
+                        int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls) {
   XiParams<C> p;
+  p.ls = ls != nullptr;
+  p.ls_in = ls ? ls->in : nullptr;
+  p.ls_chi = ls ? ls->chi : nullptr;
+  p.ls_chi_rs = ls ? ls->chi_rs : 0;
+  p.rows_rhs = make_fdiv((uint32_t)(3 * g.tc[2] * g.tc[1]));
+  p.rows_zy = make_fdiv((uint32_t)(g.tc[2] * g.tc[1]));
+  if (ls && (g.parT != 1 || axpby)) return cudaErrorInvalidValue;
   p.A = A;
   p.out = out;
   p.pl = d.plan_d[0];
@@ -1244,7 +1283,8 @@ cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const
 
 template <typename C>
 cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out,
-                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st) {
+                                C* A, C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st,
+                                const LsEpi<C>* ls) {
   cudaError_t e;
   const Work w = work_sizes(g);
   const int64_t nq_slab = w.slab_planes;
@@ -1274,7 +1314,7 @@ cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, con
       const int64_t nq = (span - q0) < nq_slab ? (span - q0) : nq_slab;
       if ((e = launch_y<C>(g, d, L, true, B + r * w.b_rhs, A, q0, nq, 0, q0, st)) != cudaSuccess) return e;
       const int64_t g_off = (r * inv_planes + q0) * g.tc[1];
-      if ((e = launch_xinv<C>(g, d, L, A, out, nq * g.tc[1], g_off, axpby, alpha, beta, st)) != cudaSuccess)
+      if ((e = launch_xinv<C>(g, d, L, A, out, nq * g.tc[1], g_off, axpby, alpha, beta, st, ls)) != cudaSuccess)
         return e;
     }
   return cudaSuccess;
@@ -1282,9 +1322,9 @@ cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, con
 
 template <typename C>
 cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A, C* B,
-                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st) {
+                          int nrhs, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls) {
   for (int ph = 0; ph < 3; ++ph) {
-    cudaError_t e = launch_matvec_phase<C>(ph, g, d, L, in, out, A, B, nrhs, axpby, alpha, beta, st);
+    cudaError_t e = launch_matvec_phase<C>(ph, g, d, L, in, out, A, B, nrhs, axpby, alpha, beta, st, ls);
     if (e != cudaSuccess) return e;
   }
   return cudaSuccess;
@@ -1292,15 +1332,15 @@ cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, con
 
 #define GILA_INST(C)                                                                                              \
   template cudaError_t launch_matvec_phase<C>(int, const Geom&, const DevOp<C>&, const Launch&, const C*, C*, C*, \
-                                              C*, int, bool, C, C, cudaStream_t);                                 \
+                                              C*, int, bool, C, C, cudaStream_t, const LsEpi<C>*);                                 \
   template cudaError_t launch_matvec<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, C*, C*, int,   \
-                                        bool, C, C, cudaStream_t);                                                \
+                                        bool, C, C, cudaStream_t, const LsEpi<C>*);                                                \
   template cudaError_t launch_xfwd<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
                                       cudaStream_t);                                                              \
   template cudaError_t launch_y<C>(const Geom&, const DevOp<C>&, const Launch&, bool, const C*, C*, int64_t,      \
                                    int64_t, int64_t, int64_t, cudaStream_t);                                      \
   template cudaError_t launch_z<C>(const Geom&, const DevOp<C>&, const Launch&, C*, int, cudaStream_t);           \
   template cudaError_t launch_xinv<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
-                                      int64_t, bool, C, C, cudaStream_t);
+                                      int64_t, bool, C, C, cudaStream_t, const LsEpi<C>*);
 
 }  // namespace gila

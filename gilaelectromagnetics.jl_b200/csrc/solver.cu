@@ -116,36 +116,77 @@ __device__ __forceinline__ void block_sum_store(const double2 (&acc)[KM], int k,
 }
 
 // ------------------------------------------------------------ reductions
-// part[r][0][blk] = sum_i conj(a_r[i]) b_r[i]  (a_rs = 0: one a for all r)
-template <typename CA, typename CB>
-__global__ void __launch_bounds__(kT) k_dot(const CA* __restrict__ a, int64_t a_rs, const CB* __restrict__ b,
-                                            int64_t n, double2* __restrict__ part) {
+// W complex values per 16-byte transaction: FP32 vectors move two values
+// (float4) per load / store, FP64 one; W = 2 needs an even n (host-checked).
+template <typename C, int W>
+struct VIO;
+template <>
+struct VIO<float2, 2> {
+  __device__ __forceinline__ static void ld(const float2* p, int64_t u, double2 (&v)[2]) {
+    const float4 q = reinterpret_cast<const float4*>(p)[u];
+    v[0] = make_double2(q.x, q.y);
+    v[1] = make_double2(q.z, q.w);
+  }
+  __device__ __forceinline__ static void st(float2* p, int64_t u, const double2 (&v)[2]) {
+    reinterpret_cast<float4*>(p)[u] = make_float4((float)v[0].x, (float)v[0].y, (float)v[1].x, (float)v[1].y);
+  }
+};
+template <typename C>
+struct VIO<C, 1> {
+  __device__ __forceinline__ static void ld(const C* p, int64_t u, double2 (&v)[1]) { v[0] = to_d(p[u]); }
+  __device__ __forceinline__ static void st(C* p, int64_t u, const double2 (&v)[1]) { p[u] = from_d<C>(v[0]); }
+};
+// the value a store of v leaves in memory (rounded to C)
+template <typename C>
+__device__ __forceinline__ double2 rounded(double2 v) {
+  return to_d(from_d<C>(v));
+}
+
+// part[r][0][blk] = sum_i conj(shadow[i]) b_r[i] over W-value units
+template <typename C, int W>
+__global__ void __launch_bounds__(kT) k_sdot(const C* __restrict__ a, const C* __restrict__ b, int64_t n,
+                                             double2* __restrict__ part) {
   const int r = blockIdx.y, nb = gridDim.x;
-  a += a_rs * r;
   b += n * r;
   double2 acc[1] = {make_double2(0.0, 0.0)};
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT)
-    acc[0] = cadd(acc[0], cjmul(to_d(a[i]), to_d(b[i])));
+  const int64_t nu = n / W;
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)nb * kT) {
+    double2 x[W], y[W];
+    VIO<C, W>::ld(a, u, x);
+    VIO<C, W>::ld(b, u, y);
+#pragma unroll
+    for (int w = 0; w < W; ++w) acc[0] = cadd(acc[0], cjmul(x[w], y[w]));
+  }
   block_sum_store<1>(acc, 1, part + (int64_t)r * nb + blockIdx.x, nb);
 }
 
 // Gram matrix r_a^H r_b, a <= b <= ell, of the MR step (all kGram slots).
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_gram(KVec<C> v, int ell, int64_t n, double2* __restrict__ part) {
   const int r = blockIdx.y, nb = gridDim.x;
-  const int64_t off = (int64_t)r * n;
+  const int64_t off = (int64_t)r * n / W;
   double2 acc[kGram];
 #pragma unroll
   for (int k = 0; k < kGram; ++k) acc[k] = make_double2(0.0, 0.0);
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT) {
-    double2 e[kMaxEll + 1];
+  const int64_t nu = n / W;
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)nb * kT) {
+    double2 e[kMaxEll + 1][W];
 #pragma unroll
-    for (int a = 0; a <= kMaxEll; ++a) e[a] = a <= ell ? to_d(v.r[a][off + i]) : make_double2(0.0, 0.0);
+    for (int a = 0; a <= kMaxEll; ++a) {
+      if (a <= ell) {
+        VIO<C, W>::ld(v.r[a], off + u, e[a]);
+      } else {
+#pragma unroll
+        for (int w = 0; w < W; ++w) e[a][w] = make_double2(0.0, 0.0);
+      }
+    }
 #pragma unroll
     for (int a = 0; a <= kMaxEll; ++a)
 #pragma unroll
       for (int b = a; b <= kMaxEll; ++b)
-        if (b <= ell) acc[gidx(a, b)] = cadd(acc[gidx(a, b)], cjmul(e[a], e[b]));
+        if (b <= ell)
+#pragma unroll
+          for (int w = 0; w < W; ++w) acc[gidx(a, b)] = cadd(acc[gidx(a, b)], cjmul(e[a][w], e[b][w]));
   }
   block_sum_store<kGram>(acc, kGram, part + (int64_t)r * kGram * nb + blockIdx.x, nb);
 }
@@ -276,18 +317,26 @@ __global__ void k_mr_solve(double2* sc, Stat* st, int ell, int nrhs) {
 }
 
 // ------------------------------------------------------- vector updates
+// (all over W-value units; off = the slot's offset in units)
 // BiCG part, step j (1-based): u_q = r_q - beta u_q, q < j, beta = rho / sigma
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_bicg_u(KVec<C> v, int j, int64_t n, const double2* __restrict__ sc,
                                                const Stat* __restrict__ st) {
   const int r = blockIdx.y;
   if (!st[r].act) return;
   const double2 beta = cdiv(sc[(int64_t)r * kSlots + S_RHO], sc[(int64_t)r * kSlots + S_SIG]);
-  const int64_t off = (int64_t)r * n;
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT)
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)gridDim.x * kT)
 #pragma unroll
     for (int q = 0; q < kMaxEll; ++q)
-      if (q < j) v.u[q][off + i] = from_d<C>(csub(to_d(v.r[q][off + i]), cmul(beta, to_d(v.u[q][off + i]))));
+      if (q < j) {
+        double2 a[W], b[W];
+        VIO<C, W>::ld(v.r[q], off + u, a);
+        VIO<C, W>::ld(v.u[q], off + u, b);
+#pragma unroll
+        for (int w = 0; w < W; ++w) b[w] = csub(a[w], cmul(beta, b[w]));
+        VIO<C, W>::st(v.u[q], off + u, b);
+      }
 }
 
 // BiCG part, step j: r_q -= alpha u_{q+1}, q < j; x += alpha u_0; alpha =
@@ -295,30 +344,41 @@ __global__ void __launch_bounds__(kT) k_bicg_u(KVec<C> v, int j, int64_t n, cons
 // already brought to tolerance ends the solve there: continuing the cycle
 // would divide rounding noise by rounding noise (sigma of the next step is
 // rho - beta * rho_prev; with chi = 0 the first step converges exactly).
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_bicg_r(KVec<C> v, int j, int64_t n, const double2* __restrict__ sc,
                                                const Stat* __restrict__ st, double2* __restrict__ part) {
   const int r = blockIdx.y, nb = gridDim.x;
   if (!st[r].act) return;
   const double2 alpha = cdiv(sc[(int64_t)r * kSlots + S_RHO], sc[(int64_t)r * kSlots + S_SIG]);
-  const int64_t off = (int64_t)r * n;
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
   double2 acc[1] = {make_double2(0.0, 0.0)};
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT) {
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)nb * kT) {
 #pragma unroll
     for (int q = 0; q < kMaxEll; ++q)
       if (q < j) {
-        const C t = from_d<C>(csub(to_d(v.r[q][off + i]), cmul(alpha, to_d(v.u[q + 1][off + i]))));
-        v.r[q][off + i] = t;
-        if (q == 0) acc[0].x += cabs2(to_d(t));
+        double2 a[W], b[W];
+        VIO<C, W>::ld(v.r[q], off + u, a);
+        VIO<C, W>::ld(v.u[q + 1], off + u, b);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          a[w] = csub(a[w], cmul(alpha, b[w]));
+          if (q == 0) acc[0].x += cabs2(rounded<C>(a[w]));
+        }
+        VIO<C, W>::st(v.r[q], off + u, a);
       }
-    v.x[off + i] = from_d<C>(cadd(to_d(v.x[off + i]), cmul(alpha, to_d(v.u[0][off + i]))));
+    double2 x[W], u0[W];
+    VIO<C, W>::ld(v.x, off + u, x);
+    VIO<C, W>::ld(v.u[0], off + u, u0);
+#pragma unroll
+    for (int w = 0; w < W; ++w) x[w] = cadd(x[w], cmul(alpha, u0[w]));
+    VIO<C, W>::st(v.x, off + u, x);
   }
   block_sum_store<1>(acc, 1, part + (int64_t)r * nb + blockIdx.x, nb);
 }
 
 // MR part: u_0 -= sum_k gamma_k u_k, x += sum_k gamma_k r_{k-1},
 // r_0 -= sum_k gamma_k r_k (k = 1..l), and the partial of |r_0|^2.
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_mr_update(KVec<C> v, int ell, int64_t n, const double2* __restrict__ sc,
                                                   const Stat* __restrict__ st, double2* __restrict__ part) {
   const int r = blockIdx.y, nb = gridDim.x;
@@ -327,48 +387,35 @@ __global__ void __launch_bounds__(kT) k_mr_update(KVec<C> v, int ell, int64_t n,
 #pragma unroll
   for (int k = 0; k < kMaxEll; ++k)
     g[k] = k < ell ? sc[(int64_t)r * kSlots + S_GAM + k] : make_double2(0.0, 0.0);
-  const int64_t off = (int64_t)r * n;
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
   double2 acc[1] = {make_double2(0.0, 0.0)};
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)nb * kT) {
-    double2 u0 = to_d(v.u[0][off + i]), r0 = to_d(v.r[0][off + i]), x = to_d(v.x[off + i]);
-    x = cadd(x, cmul(g[0], r0));
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)nb * kT) {
+    double2 u0[W], r0[W], x[W];
+    VIO<C, W>::ld(v.u[0], off + u, u0);
+    VIO<C, W>::ld(v.r[0], off + u, r0);
+    VIO<C, W>::ld(v.x, off + u, x);
+#pragma unroll
+    for (int w = 0; w < W; ++w) x[w] = cadd(x[w], cmul(g[0], r0[w]));
 #pragma unroll
     for (int k = 1; k <= kMaxEll; ++k)
       if (k <= ell) {
-        const double2 rk = to_d(v.r[k][off + i]);
-        u0 = csub(u0, cmul(g[k - 1], to_d(v.u[k][off + i])));
-        r0 = csub(r0, cmul(g[k - 1], rk));
-        if (k < ell) x = cadd(x, cmul(g[k], rk));
+        double2 rk[W], uk[W];
+        VIO<C, W>::ld(v.r[k], off + u, rk);
+        VIO<C, W>::ld(v.u[k], off + u, uk);
+#pragma unroll
+        for (int w = 0; w < W; ++w) {
+          u0[w] = csub(u0[w], cmul(g[k - 1], uk[w]));
+          r0[w] = csub(r0[w], cmul(g[k - 1], rk[w]));
+          if (k < ell) x[w] = cadd(x[w], cmul(g[k], rk[w]));
+        }
       }
-    v.u[0][off + i] = from_d<C>(u0);
-    v.r[0][off + i] = from_d<C>(r0);
-    v.x[off + i] = from_d<C>(x);
-    const double2 r0s = to_d(from_d<C>(r0));
-    acc[0].x += cabs2(r0s);
+    VIO<C, W>::st(v.u[0], off + u, u0);
+    VIO<C, W>::st(v.r[0], off + u, r0);
+    VIO<C, W>::st(v.x, off + u, x);
+#pragma unroll
+    for (int w = 0; w < W; ++w) acc[0].x += cabs2(rounded<C>(r0[w]));
   }
   block_sum_store<1>(acc, 1, part + (int64_t)r * nb + blockIdx.x, nb);
-}
-
-// Lippmann-Schwinger combine after out = G in: out = in - chi .* out, chi per
-// cell broadcast over the three components (examples/GilaOperators.jl:94);
-// chi_rs = 0: one medium for all right-hand sides, V: one per right-hand side.
-template <typename C>
-__global__ void __launch_bounds__(kT) k_ls_combine(const C* __restrict__ in, C* __restrict__ out,
-                                                   const C* __restrict__ chi, int64_t chi_rs, int64_t V,
-                                                   const Stat* __restrict__ st) {
-  const int r = blockIdx.y;
-  if (st && !st[r].act) return;
-  in += 3 * V * r;
-  out += 3 * V * r;
-  chi += chi_rs * r;
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < V; i += (int64_t)gridDim.x * kT) {
-    const double2 c = to_d(chi[i]);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) {
-      const int64_t j = q * V + i;
-      out[j] = from_d<C>(csub(to_d(in[j]), cmul(c, to_d(out[j]))));
-    }
-  }
 }
 
 // ------------------------------------------------- refinement (FP64) steps
@@ -399,54 +446,73 @@ __global__ void __launch_bounds__(kT) k_resid(const double2* __restrict__ b, con
 // (Re)start of the Krylov process on the scaled correction equation
 // A d = r / s for the masked right-hand sides: r_0 = r64 * inv (inv = 1/s,
 // rounded to C), d = 0, u_0 = 0.
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_inner_start(const double2* __restrict__ r64, KVec<C> v,
                                                     const double* __restrict__ inv, const int* __restrict__ mask,
                                                     int64_t n) {
   const int r = blockIdx.y;
   if (!mask[r]) return;
   const double s = inv[r];
-  const int64_t off = (int64_t)r * n;
-  const C zero = from_d<C>(make_double2(0.0, 0.0));
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
-    const double2 a = r64[off + i];
-    v.r[0][off + i] = from_d<C>(make_double2(a.x * s, a.y * s));
-    v.u[0][off + i] = zero;
-    v.x[off + i] = zero;
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
+  double2 z[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) z[w] = make_double2(0.0, 0.0);
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)gridDim.x * kT) {
+    double2 a[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const double2 q = r64[(off + u) * W + w];
+      a[w] = make_double2(q.x * s, q.y * s);
+    }
+    VIO<C, W>::st(v.r[0], off + u, a);
+    VIO<C, W>::st(v.u[0], off + u, z);
+    VIO<C, W>::st(v.x, off + u, z);
   }
 }
 
 // Reliable update, first half: x64 += s * d and d = 0 for the masked
 // right-hand sides (the correction leaves the low-precision iterate).
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_accum(double2* __restrict__ x, C* __restrict__ d,
                                               const double* __restrict__ scale, const int* __restrict__ mask,
                                               int64_t n) {
   const int r = blockIdx.y;
   if (!mask[r]) return;
   const double s = scale[r];
-  const int64_t off = (int64_t)r * n;
-  const C zero = from_d<C>(make_double2(0.0, 0.0));
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
-    const double2 a = to_d(d[off + i]);
-    x[off + i] = make_double2(x[off + i].x + s * a.x, x[off + i].y + s * a.y);
-    d[off + i] = zero;
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
+  double2 z[W];
+#pragma unroll
+  for (int w = 0; w < W; ++w) z[w] = make_double2(0.0, 0.0);
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)gridDim.x * kT) {
+    double2 a[W];
+    VIO<C, W>::ld(d, off + u, a);
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      double2& xv = x[(off + u) * W + w];
+      xv = make_double2(xv.x + s * a[w].x, xv.y + s * a[w].y);
+    }
+    VIO<C, W>::st(d, off + u, z);
   }
 }
 
 // Reliable update, second half: the recursive residual of the masked
 // right-hand sides is replaced by the FP64 one, r_0 = (b - A64 x) * inv.
-template <typename C>
+template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_replace(const double2* __restrict__ r64, C* __restrict__ r0,
                                                 const double* __restrict__ inv, const int* __restrict__ mask,
                                                 int64_t n) {
   const int r = blockIdx.y;
   if (!mask[r]) return;
   const double s = inv[r];
-  const int64_t off = (int64_t)r * n;
-  for (int64_t i = (int64_t)blockIdx.x * kT + threadIdx.x; i < n; i += (int64_t)gridDim.x * kT) {
-    const double2 a = r64[off + i];
-    r0[off + i] = from_d<C>(make_double2(a.x * s, a.y * s));
+  const int64_t off = (int64_t)r * n / W, nu = n / W;
+  for (int64_t u = (int64_t)blockIdx.x * kT + threadIdx.x; u < nu; u += (int64_t)gridDim.x * kT) {
+    double2 a[W];
+#pragma unroll
+    for (int w = 0; w < W; ++w) {
+      const double2 q = r64[(off + u) * W + w];
+      a[w] = make_double2(q.x * s, q.y * s);
+    }
+    VIO<C, W>::st(r0, off + u, a);
   }
 }
 
@@ -545,12 +611,25 @@ struct OpRef {  // an operator with workspaces owned by a batch
 // updates are rare, so their matvecs run in chunks
 constexpr int kUpdateCap = 4;
 
+// the Krylov-vector kernels in W-value units: FP32 vectors of even length
+// move two values per 16-byte access
+#define GILA_VW(KERNEL, GRID, ...)                                        \
+  do {                                                                    \
+    if (w2_)                                                              \
+      KERNEL<CI, kW2><<<GRID, kT, 0, s_>>>(__VA_ARGS__);                  \
+    else                                                                  \
+      KERNEL<CI, 1><<<GRID, kT, 0, s_>>>(__VA_ARGS__);                    \
+  } while (0)
+
 template <typename CI>
 class LsBatchT final : public LsBatch {
+  static constexpr int kW2 = sizeof(CI) == 8 ? 2 : 1;
+
  public:
   LsBatchT(Core& a, Core& i, int S, const BatchCfg& c)
       : g64_(a), gi_(i), S_(S), n_(in_elems(a)), V_(in_elems(a) / 3), cfg_(c), sl_(S) {
     nb_ = vec_blocks(n_);
+    w2_ = kW2 == 2 && n_ % 2 == 0;
   }
   ~LsBatchT() override {
     if (s_) cudaStreamSynchronize(s_);
@@ -820,16 +899,21 @@ class LsBatchT final : public LsBatch {
     return GILA_OK;
   }
 
+  // out = G in over runs of the slots in m; with chi, the Lippmann-Schwinger
+  // epilogue out = in - chi .* (G in) runs in the matvec's last pass
   template <typename C>
-  gila_status apply_runs(const OpRef<C>& op, const C* in, C* out, const std::vector<char>& m) {
+  gila_status apply_runs(const OpRef<C>& op, const C* in, C* out, const std::vector<char>& m,
+                         const C* chi = nullptr) {
     C one, zero;  // host side: no device helpers here
     one.x = 1;
     one.y = 0;
     zero.x = 0;
     zero.y = 0;
     for (auto [r0, r1] : runs_of(m, op.cap)) {
+      LsEpi<C> ep{in + (size_t)r0 * n_, chi ? chi + (size_t)r0 * chi_rs() : nullptr, chi_rs()};
       GILA_CUDA_TRY(launch_matvec<C>(op.geom, devop<C>(*op.core), op.core->launch, in + (size_t)r0 * n_,
-                                     out + (size_t)r0 * n_, op.A, op.B, r1 - r0, false, one, zero, s_));
+                                     out + (size_t)r0 * n_, op.A, op.B, r1 - r0, false, one, zero, s_,
+                                     chi ? &ep : nullptr));
     }
     return GILA_OK;
   }
@@ -927,7 +1011,7 @@ class LsBatchT final : public LsBatch {
     gila_status st;
     if ((st = upload_params()) != GILA_OK) return st;
     if ((st = upload_status()) != GILA_OK) return st;
-    k_inner_start<CI><<<dim3(nb_, S_), kT, 0, s_>>>(r64_, kv_, pd(2), mask_d(), n_);
+    GILA_VW(k_inner_start, dim3(nb_, S_), r64_, kv_, pd(2), mask_d(), n_);
     k_scal_init<<<(S_ + 127) / 128, 128, 0, s_>>>(sc_, mask_d(), S_);
     GILA_CUDA_TRY(cudaGetLastError());
     return GILA_OK;
@@ -942,30 +1026,25 @@ class LsBatchT final : public LsBatch {
     double* tol2 = pd(0);
     gila_status st;
     const int ell = cfg_.ell;
-    auto lsa = [&](const CI* in, CI* out) -> gila_status {
-      gila_status s2 = apply_runs<CI>(opi_, in, out, m);
-      if (s2 != GILA_OK) return s2;
-      k_ls_combine<CI><<<gv, kT, 0, s_>>>(in, out, chii_, chi_rs(), V_, st_d_);
-      return GILA_OK;
-    };
+    auto lsa = [&](const CI* in, CI* out) -> gila_status { return apply_runs<CI>(opi_, in, out, m, chii_); };
     k_iter_start<<<sb, 128, 0, s_>>>(sc_, st_d_, S_);
     for (int j = 1; j <= ell; ++j) {
-      k_dot<CI, CI><<<gv, kT, 0, s_>>>(shadow_, 0, kv_.r[j - 1], n_, part_);
+      GILA_VW(k_sdot, gv, shadow_, kv_.r[j - 1], n_, part_);
       k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_RHO, st_d_, tol2, FIN_CHECK);
-      k_bicg_u<CI><<<gv, kT, 0, s_>>>(kv_, j, n_, sc_, st_d_);
+      GILA_VW(k_bicg_u, gv, kv_, j, n_, sc_, st_d_);
       GILA_CUDA_TRY(cudaGetLastError());
       if ((st = lsa(kv_.u[j - 1], kv_.u[j])) != GILA_OK) return st;
-      k_dot<CI, CI><<<gv, kT, 0, s_>>>(shadow_, 0, kv_.u[j], n_, part_);
+      GILA_VW(k_sdot, gv, shadow_, kv_.u[j], n_, part_);
       k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_SIG, st_d_, tol2, FIN_CHECK);
-      k_bicg_r<CI><<<gv, kT, 0, s_>>>(kv_, j, n_, sc_, st_d_, part_);
+      GILA_VW(k_bicg_r, gv, kv_, j, n_, sc_, st_d_, part_);
       k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
       GILA_CUDA_TRY(cudaGetLastError());
       if ((st = lsa(kv_.r[j - 1], kv_.r[j])) != GILA_OK) return st;
     }
-    k_gram<CI><<<gv, kT, 0, s_>>>(kv_, ell, n_, part_);
+    GILA_VW(k_gram, gv, kv_, ell, n_, part_);
     k_fin<<<S_, kT, 0, s_>>>(part_, kGram, nb_, sc_, S_GRAM, st_d_, tol2, FIN_STORE);
     k_mr_solve<<<sb, 128, 0, s_>>>(sc_, st_d_, ell, S_);
-    k_mr_update<CI><<<gv, kT, 0, s_>>>(kv_, ell, n_, sc_, st_d_, part_);
+    GILA_VW(k_mr_update, gv, kv_, ell, n_, sc_, st_d_, part_);
     k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
     GILA_CUDA_TRY(cudaGetLastError());
     GILA_CUDA_TRY(cudaMemcpyAsync(st_h_, st_d_, (size_t)S_ * sizeof(Stat), cudaMemcpyDeviceToHost, s_));
@@ -1052,10 +1131,10 @@ class LsBatchT final : public LsBatch {
     if (!any) return GILA_OK;
     gila_status st;
     if ((st = upload_params()) != GILA_OK) return st;
-    k_accum<CI><<<dim3(nb_, S_), kT, 0, s_>>>(x64_, kv_.x, pd(1), mask_d(), n_);
+    GILA_VW(k_accum, dim3(nb_, S_), x64_, kv_.x, pd(1), mask_d(), n_);
     GILA_CUDA_TRY(cudaGetLastError());
     if ((st = true_residual(m)) != GILA_OK) return st;
-    k_replace<CI><<<dim3(nb_, S_), kT, 0, s_>>>(r64_, kv_.r[0], pd(2), mask_d(), n_);
+    GILA_VW(k_replace, dim3(nb_, S_), r64_, kv_.r[0], pd(2), mask_d(), n_);
     GILA_CUDA_TRY(cudaGetLastError());
     ++inf_.outer;
     *upd = true;
@@ -1100,6 +1179,7 @@ class LsBatchT final : public LsBatch {
   int64_t n_, V_;
   BatchCfg cfg_;
   int nb_ = 1;
+  bool w2_ = false;
   cudaStream_t s_ = nullptr;
   cudaEvent_t ev_ = nullptr;
   struct Arena : DevArena {
