@@ -163,8 +163,10 @@ __device__ __forceinline__ void ct_run(const C* __restrict__ tw, const LdF& ld_f
 // a task handles two adjacent lines, so each shared-memory access moves both
 // lines' values in one 16-byte transaction and the two lines share the
 // twiddles and the index arithmetic.  M2 = line pairs; ld / st take a pair
-// index and a position and move float4 = (line 2p, line 2p + 1).
-template <int P, int S, int T, int M2, bool INV, bool REV, class Ld, class St>
+// index and a position and move float4 = (line 2p, line 2p + 1).  LF: pairs
+// fastest across threads (y, z layouts [index][pair]) or positions fastest
+// (x layout [pair][index]).
+template <int P, int S, int T, int M2, bool INV, bool REV, bool LF, class Ld, class St>
 __device__ __forceinline__ void ct_stage2(const float2* __restrict__ tw, const Ld& ld, const St& st, bool sync_mid) {
   constexpr int R = ct_radix_o<REV>(P, S);
   constexpr int NS = ct_span_o<REV>(P, S);
@@ -177,7 +179,7 @@ __device__ __forceinline__ void ct_stage2(const float2* __restrict__ tw, const L
   for (int k = 0; k < K; ++k) {
     const int task = (int)threadIdx.x + k * T;
     if (NTASK % T == 0 || task < NTASK) {
-      const int lp = task % M2, j = task / M2;
+      const int lp = LF ? task % M2 : task / TPL, j = LF ? task / M2 : task % TPL;
 #pragma unroll
       for (int r = 0; r < R; ++r) {
         const float4 q = ld(lp, j + r * TPL);
@@ -191,7 +193,7 @@ __device__ __forceinline__ void ct_stage2(const float2* __restrict__ tw, const L
   for (int k = 0; k < K; ++k) {
     const int task = (int)threadIdx.x + k * T;
     if (NTASK % T == 0 || task < NTASK) {
-      const int lp = task % M2, j = task / M2;
+      const int lp = LF ? task % M2 : task / TPL, j = LF ? task / M2 : task % TPL;
       const int jm = j % NS;
       if (NS > 1) {
         float2 w[R];
@@ -212,7 +214,8 @@ __device__ __forceinline__ void ct_stage2(const float2* __restrict__ tw, const L
   }
 }
 
-template <int P, int S0, int S, int S1, int T, int M2, bool INV, bool REV, class LdF, class LdM, class StM, class StL>
+template <int P, int S0, int S, int S1, int T, int M2, bool INV, bool REV, bool LF, class LdF, class LdM, class StM,
+          class StL>
 __device__ __forceinline__ void ct_run_range2(const float2* __restrict__ tw, const LdF& ld_first, const LdM& ld_mid,
                                               const StM& st_mid, const StL& st_last, bool first_in_smem,
                                               bool last_in_smem) {
@@ -220,16 +223,16 @@ __device__ __forceinline__ void ct_run_range2(const float2* __restrict__ tw, con
     constexpr bool first = (S == S0), last = (S == S1 - 1);
     const bool sync_mid = (first ? first_in_smem : true) && (last ? last_in_smem : true);
     if constexpr (first && last)
-      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_first, st_last, sync_mid);
+      ct_stage2<P, S, T, M2, INV, REV, LF>(tw, ld_first, st_last, sync_mid);
     else if constexpr (first)
-      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_first, st_mid, sync_mid);
+      ct_stage2<P, S, T, M2, INV, REV, LF>(tw, ld_first, st_mid, sync_mid);
     else if constexpr (last)
-      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_mid, st_last, sync_mid);
+      ct_stage2<P, S, T, M2, INV, REV, LF>(tw, ld_mid, st_last, sync_mid);
     else
-      ct_stage2<P, S, T, M2, INV, REV>(tw, ld_mid, st_mid, sync_mid);
+      ct_stage2<P, S, T, M2, INV, REV, LF>(tw, ld_mid, st_mid, sync_mid);
     __syncthreads();
-    ct_run_range2<P, S0, S + 1, S1, T, M2, INV, REV>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem,
-                                                     last_in_smem);
+    ct_run_range2<P, S0, S + 1, S1, T, M2, INV, REV, LF>(tw, ld_first, ld_mid, st_mid, st_last, first_in_smem,
+                                                         last_in_smem);
   }
 }
 

@@ -444,6 +444,97 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd
   ct_run<C, P, 8, T, M, false, false>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
+// FP32 x passes on row pairs: rows 2p and 2p+1 interleaved in shared memory
+// (float4 slot = element i of both rows, slot i + i/8 of the pair's row), so
+// every stage access is a conflict-free 16-byte transaction -- the access
+// pattern of the FP64 passes -- and the two rows share twiddles.
+template <int P>
+__global__ void __launch_bounds__(ct_threads2(ct_xlines<8>(P), P)) k_xfwd2_ct(const XfParams<float2> p) {
+  constexpr int M = ct_xlines<8>(P);  // rows per CTA (even for the lengths compiled)
+  constexpr int M2 = M / 2;
+  constexpr int T = ct_threads2(M, P);
+  constexpr int LS = P + (P + 7) / 8;  // float4 slots per pair row
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int nin = p.nin;
+  const int64_t rows = p.rows;
+  float2* const A = p.A;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
+  {
+    // consecutive threads fill the two halves of consecutive slots
+    const float2* const src = p.in + g0 * nin;
+    for (int q = threadIdx.x; q < M2 * 2 * nin; q += T) {
+      const int pr = q / (2 * nin), rem = q - pr * 2 * nin;
+      const int i = rem >> 1, h = rem & 1;
+      const int l = 2 * pr + h;
+      if (l < nl) cp_async(reinterpret_cast<float2*>(sm + pr * LS + i + (i >> 3)) + h, src + (int64_t)l * nin + i);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+  auto ldf = [=](int lp, int i) -> float4 {
+    if (i < nin) return sm[lp * LS + i + (i >> 3)];
+    return z4;
+  };
+  auto lds = [=](int lp, int i) -> float4 { return sm[lp * LS + i + (i >> 3)]; };
+  auto sts = [=](int lp, int i, float4 v) { sm[lp * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int lp, int i, float4 v) {
+    const int64_t g = g0 + 2 * lp;
+    if (g < rows) A[g * P + i] = make_float2(v.x, v.y);
+    if (g + 1 < rows) A[(g + 1) * P + i] = make_float2(v.z, v.w);
+  };
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, false, false, false>(p.tw, ldf, lds, sts, stg, true, false);
+}
+
+template <int P>
+__global__ void __launch_bounds__(ct_threads2(ct_xlines<8>(P), P)) k_xinv2_ct(const XiParams<float2> p) {
+  constexpr int M = ct_xlines<8>(P);
+  constexpr int M2 = M / 2;
+  constexpr int T = ct_threads2(M, P);
+  constexpr int LS = P + (P + 7) / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int nout = p.nout;
+  const int64_t rows = p.rows;
+  float2* const out = p.out;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const int64_t g_off = p.g_off;
+  const int ls = p.ls;
+  const float2* const ls_in = p.ls_in;
+  const float2* const ls_chi = p.ls_chi;
+  const int64_t ls_chi_rs = p.ls_chi_rs;
+  const FDiv rows_rhs = p.rows_rhs, rows_zy = p.rows_zy;
+  const int nl = (int)((rows - g0) < M ? (rows - g0) : M);
+  {
+    const float2* const src = p.A + g0 * P;
+    for (int q = threadIdx.x; q < M2 * 2 * P; q += T) {
+      const int pr = q / (2 * P), rem = q - pr * 2 * P;
+      const int i = rem >> 1, h = rem & 1;
+      const int l = 2 * pr + h;
+      if (l < nl) cp_async(reinterpret_cast<float2*>(sm + pr * LS + i + (i >> 3)) + h, src + (int64_t)l * P + i);
+    }
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  auto lds = [=](int lp, int i) -> float4 { return sm[lp * LS + i + (i >> 3)]; };
+  auto sts = [=](int lp, int i, float4 v) { sm[lp * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int lp, int i, float4 v) {
+    if (i >= nout) return;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t g = g0 + 2 * lp + h;
+      if (g >= rows) return;
+      const int64_t gg = g + g_off;
+      const int64_t o = gg * nout + i;
+      const float2 w = h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+      out[o] = ls ? ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, w) : w;
+    }
+  };
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, true, false, false>(p.tw, lds, lds, sts, stg, true, false);
+}
+
 template <typename C, int P, bool INV, int TX>
 __global__ void __launch_bounds__(ct_threads(TX, P)) k_y_ct(const YParams<C> p) {
   constexpr int T = ct_threads(TX, P);
@@ -508,7 +599,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P)) k_y2_ct(const YParams<floa
   auto stg = [=](int t2, int i, float4 v) {
     if (2 * t2 < tmax && i < nout) reinterpret_cast<float4*>(dst + (int64_t)i * Px)[t2] = v;
   };
-  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, INV, false>(p.tw, ldf, lds, sts, stg, true, false);
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, INV, false, true>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
 template <typename C, int P, int TX>
@@ -812,7 +903,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf_min_bloc
     };
     auto lds = [=](int t2, int i) -> float4 { return smc[i * M2 + t2]; };
     auto sts = [=](int t2, int i, float4 v) { smc[i * M2 + t2] = v; };
-    ct_run_range2<P, 0, 0, NST - 1, T, M2, false, false>(p.tw, ldf, lds, sts, sts, true, true);
+    ct_run_range2<P, 0, 0, NST - 1, T, M2, false, false, true>(p.tw, ldf, lds, sts, sts, true, true);
   }
   int py, iy, ry;
   ax_map(p.ax[1], ky, py, iy, ry);
@@ -895,7 +986,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf_min_bloc
     auto stg = [=](int t2, int i, float4 v) {
       if (2 * t2 < tmax && i < nout) reinterpret_cast<float4*>(Bo + (int64_t)i * plane)[t2] = v;
     };
-    ct_run_range2<P, 1, 1, NST, T, M2, true, true>(p.tw, ldp, ldo, sto, stg, true, false);
+    ct_run_range2<P, 1, 1, NST, T, M2, true, true, true>(p.tw, ldp, ldo, sto, stg, true, false);
   }
 }
 
@@ -997,6 +1088,14 @@ template <typename C>
 static inline const YParams<float2>& yp32(const YParams<C>& p) {
   return reinterpret_cast<const YParams<float2>&>(p);
 }
+template <typename C>
+static inline const XfParams<float2>& xfp32(const XfParams<C>& p) {
+  return reinterpret_cast<const XfParams<float2>&>(p);
+}
+template <typename C>
+static inline const XiParams<float2>& xip32(const XiParams<C>& p) {
+  return reinterpret_cast<const XiParams<float2>&>(p);
+}
 
 static cudaError_t set_smem(const void* fn, size_t bytes) {
   if (bytes > 48 * 1024) return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
@@ -1032,6 +1131,19 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
   p.nind = make_fdiv((uint32_t)p.nin);
   if (ct_has(p.P)) {
 #define GILA_CT_XF(n)                                                                  \
+  if constexpr (sizeof(C) == 8) {                                                      \
+    if (p.P == n && zpair()) {                                                         \
+      constexpr int M = ct_xlines<8>(n);                                               \
+      const int T2 = ct_threads2(M, n);                                                \
+      const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                         \
+      p.M = M;                                                                         \
+      const int64_t blocks = (p.rows + M - 1) / M;                                     \
+      cudaError_t e2 = set_smem((const void*)k_xfwd2_ct<n>, sm);                       \
+      if (e2 != cudaSuccess) return e2;                                                \
+      k_xfwd2_ct<n><<<(unsigned)blocks, T2, sm, st>>>(xfp32(p));                       \
+      return cudaGetLastError();                                                       \
+    }                                                                                  \
+  }                                                                                    \
   if (p.P == n) {                                                                      \
     constexpr int M = ct_xlines<sizeof(C)>(n);                                         \
     const int T = ct_threads(M, n);                                                    \
@@ -1213,10 +1325,19 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
 template <typename C, bool AXPBY>
 static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, cudaStream_t st) {
   if (ct_has(p.P)) {
-#define GILA_CT_XI(n)                                 \
-  if (p.P == n) {                                     \
-    GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY>), p);  \
-    return cudaSuccess;                               \
+#define GILA_CT_XI(n)                                                    \
+  if constexpr (sizeof(C) == 8 && !AXPBY) {                              \
+    if (p.P == n && !p.part_scatter && zpair()) {                        \
+      const int T2 = ct_threads2(ct_xlines<8>(n), n);                    \
+      cudaError_t e2 = set_smem((const void*)k_xinv2_ct<n>, sm);         \
+      if (e2 != cudaSuccess) return e2;                                  \
+      k_xinv2_ct<n><<<(unsigned)blocks, T2, sm, st>>>(xip32(p));         \
+      return cudaSuccess;                                                \
+    }                                                                    \
+  }                                                                      \
+  if (p.P == n) {                                                        \
+    GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY>), p);                     \
+    return cudaSuccess;                                                  \
   }
     GILA_CT_SIZES(GILA_CT_XI)
 #undef GILA_CT_XI
