@@ -264,6 +264,11 @@ constexpr int ct_threads(int M, int P) {
 }
 // threads of a line-pair kernel over M lines (8 pairs of values per thread)
 constexpr int ct_threads2(int M, int P) { return ct_threads(M / 2, P); }
+// rows per CTA of an FP32 x pass on row pairs: even
+template <int CS>
+constexpr int ct_xlines2(int P) {
+  return ct_xlines<CS>(P) >= 2 ? ct_xlines<CS>(P) / 2 * 2 : 2;
+}
 // tile widths the y and z kernels are instantiated for (the autotuner picks
 // among them per operator): at most 512 threads and the shared-memory budget
 constexpr int kTileSet[3] = {4, 8, 16};

@@ -449,8 +449,8 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd
 // every stage access is a conflict-free 16-byte transaction -- the access
 // pattern of the FP64 passes -- and the two rows share twiddles.
 template <int P>
-__global__ void __launch_bounds__(ct_threads2(ct_xlines<8>(P), P)) k_xfwd2_ct(const XfParams<float2> p) {
-  constexpr int M = ct_xlines<8>(P);  // rows per CTA (even for the lengths compiled)
+__global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xfwd2_ct(const XfParams<float2> p) {
+  constexpr int M = ct_xlines2<8>(P);  // rows per CTA (even)
   constexpr int M2 = M / 2;
   constexpr int T = ct_threads2(M, P);
   constexpr int LS = P + (P + 7) / 8;  // float4 slots per pair row
@@ -489,8 +489,8 @@ __global__ void __launch_bounds__(ct_threads2(ct_xlines<8>(P), P)) k_xfwd2_ct(co
 }
 
 template <int P>
-__global__ void __launch_bounds__(ct_threads2(ct_xlines<8>(P), P)) k_xinv2_ct(const XiParams<float2> p) {
-  constexpr int M = ct_xlines<8>(P);
+__global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xinv2_ct(const XiParams<float2> p) {
+  constexpr int M = ct_xlines2<8>(P);
   constexpr int M2 = M / 2;
   constexpr int T = ct_threads2(M, P);
   constexpr int LS = P + (P + 7) / 8;
@@ -1133,7 +1133,7 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
 #define GILA_CT_XF(n)                                                                  \
   if constexpr (sizeof(C) == 8) {                                                      \
     if (p.P == n && zpair()) {                                                         \
-      constexpr int M = ct_xlines<8>(n);                                               \
+      constexpr int M = ct_xlines2<8>(n);                                              \
       const int T2 = ct_threads2(M, n);                                                \
       const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                         \
       p.M = M;                                                                         \
@@ -1328,10 +1328,13 @@ static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t 
 #define GILA_CT_XI(n)                                                    \
   if constexpr (sizeof(C) == 8 && !AXPBY) {                              \
     if (p.P == n && !p.part_scatter && zpair()) {                        \
-      const int T2 = ct_threads2(ct_xlines<8>(n), n);                    \
-      cudaError_t e2 = set_smem((const void*)k_xinv2_ct<n>, sm);         \
+      constexpr int M2r = ct_xlines2<8>(n);                              \
+      const int T2 = ct_threads2(M2r, n);                                \
+      const size_t sm2 = (size_t)M2r * row_stride(n) * sizeof(C);        \
+      const int64_t blocks2 = (p.rows + M2r - 1) / M2r;                  \
+      cudaError_t e2 = set_smem((const void*)k_xinv2_ct<n>, sm2);        \
       if (e2 != cudaSuccess) return e2;                                  \
-      k_xinv2_ct<n><<<(unsigned)blocks, T2, sm, st>>>(xip32(p));         \
+      k_xinv2_ct<n><<<(unsigned)blocks2, T2, sm2, st>>>(xip32(p));       \
       return cudaSuccess;                                                \
     }                                                                    \
   }                                                                      \
