@@ -655,7 +655,7 @@ class SolveInfo:
 
 def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, ell: int = 2,
           delta: float = 0.1, max_matvecs: int = 4000, max_restarts: int = 20, x0=None,
-          graph: bool = True, check: bool = True, stream=None):
+          graph: bool = True, check: bool = True, stream=None, keep: bool = False):
     """Solve ls * t = i (t = (1 - chi G)^-1 i, examples/scattering_film.jl:58-61)
     with BiCGStab(ell) on the GPU, for one field or a stack of nrhs fields.
 
@@ -666,7 +666,8 @@ def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, e
     b - A x whenever it fell by `delta`).  Returns (t, SolveInfo); raises
     GilaError when a right-hand side misses tol and `check` is set.  With a
     CUDA stream handle the solve is ordered after the work queued on it and
-    the stream waits for the solve."""
+    the stream waits for the solve.  keep=True leaves the solve's device state
+    resident with the operator for the next call of the same shape."""
     G = ls.greens_op
     if G.dtype != np.complex128:
         raise AssertionError("the solve needs the ComplexF64 Green operator (its residual is FP64)")
@@ -700,7 +701,8 @@ def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, e
             x[...] = np.reshape(np.asarray(x0), x.shape, order="F")
     chi = np.asfortranarray(ls.medium.astype(np.complex128))
     o = L.GilaSolveC(tol=tol, ell=ell, mixed=1 if mixed else 0, max_matvecs=max_matvecs,
-                     max_restarts=max_restarts, delta=delta, x0=0 if x0 is None else 1, no_graph=0 if graph else 1)
+                     max_restarts=max_restarts, delta=delta, x0=0 if x0 is None else 1, no_graph=0 if graph else 1,
+                     keep=1 if keep else 0)
     inf = L.GilaSolveInfoC()
     res = (ct.c_double * nrhs)()
     g32 = ls.g32().mem._h if mixed else None

@@ -49,7 +49,7 @@ class GilaSolveC(ct.Structure):
     """gila_solve_opts (include/gila_b200.h)."""
     _fields_ = [("tol", ct.c_double), ("ell", ct.c_int32), ("mixed", ct.c_int32),
                 ("max_matvecs", ct.c_int32), ("max_restarts", ct.c_int32), ("delta", ct.c_double),
-                ("x0", ct.c_int32), ("no_graph", ct.c_int32)]
+                ("x0", ct.c_int32), ("no_graph", ct.c_int32), ("keep", ct.c_int32)]
 
 
 class GilaSolveInfoC(ct.Structure):

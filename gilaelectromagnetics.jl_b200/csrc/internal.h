@@ -48,6 +48,7 @@ struct ExtInf {  // GlaExtInf (src/glaMem.jl:39-47)
 gila_status ext_inf(const Vol& trg, const Vol& src, ExtInf* out);
 
 struct Ctx;
+class LsBatch;
 
 // Device-resident operator data, shared between an operator and its adjoint.
 struct Core {
@@ -77,6 +78,10 @@ struct Core {
   bool tuned = false;
   cudaStream_t stream = nullptr;
   std::mutex mu;
+  // a solve batch kept resident between gila_ls_solve calls (opts->keep)
+  std::shared_ptr<LsBatch> ls_keep;
+  std::string ls_keep_key;
+  std::weak_ptr<Core> ls_keep_inner;  // the ComplexF32 operator the kept batch uses
   ~Core();
 };
 

@@ -761,6 +761,7 @@ class LsBatchT final : public LsBatch {
     return o;
   }
   const gila_solve_info& info() const override { return inf_; }
+  void reset_info() override { inf_ = gila_solve_info{}; }
   cudaStream_t stream() const override { return s_; }
 
   gila_status set_shared_chi(const void* chi) override {
@@ -1345,8 +1346,23 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
     inner = g32->core.get();
   }
   GILA_CUDA_TRY(cudaSetDevice(a.device));
-  std::unique_ptr<LsBatch> bt;
-  if ((s = make_ls_batch(a, inner, (int)nrhs, cfg, bt)) != GILA_OK) return s;
+  const bool keep = opts && opts->keep;
+  char key[160];
+  snprintf(key, sizeof key, "%p|%d|%d|%d|%d|%lld", (void*)inner, cfg.ell, cfg.mixed, cfg.graph, cfg.chi_shared,
+           (long long)nrhs);
+  std::shared_ptr<LsBatch> bt;
+  std::shared_ptr<Core> innerp = cfg.mixed ? g32->core : nullptr;
+  {
+    std::lock_guard<std::mutex> lk(a.mu);
+    if (a.ls_keep && a.ls_keep_key == key && a.ls_keep_inner.lock() == innerp) bt = a.ls_keep;
+    a.ls_keep.reset();  // taken (or stale); put back below when kept
+  }
+  if (!bt) {
+    std::unique_ptr<LsBatch> nb;
+    if ((s = make_ls_batch(a, inner, (int)nrhs, cfg, nb)) != GILA_OK) return s;
+    bt = std::move(nb);
+  }
+  bt->reset_info();
   cudaStream_t st = bt->stream();
   cudaStream_t user = static_cast<cudaStream_t>(stream);
   cudaEvent_t ev = nullptr;
@@ -1388,6 +1404,12 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
     cudaEventRecord(ev, st);
     cudaStreamWaitEvent(user, ev, 0);
     cudaEventDestroy(ev);
+  }
+  if (keep) {
+    std::lock_guard<std::mutex> lk(a.mu);
+    a.ls_keep = bt;
+    a.ls_keep_key = key;
+    a.ls_keep_inner = innerp;
   }
   if (info) *info = inf;
   if (rhs_res)

@@ -64,6 +64,7 @@ class LsBatch {
   virtual gila_status wait() = 0;  // block until it completes
   virtual std::vector<SlotResult> take_finished() = 0;
   virtual const gila_solve_info& info() const = 0;
+  virtual void reset_info() = 0;
   virtual cudaStream_t stream() const = 0;
 };
 

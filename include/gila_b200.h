@@ -195,6 +195,9 @@ typedef struct {
                            IterativeSolvers.bicgstabl(A, b) does) */
   int32_t no_graph;     /* 1: launch every Krylov cycle's kernels directly instead of replaying
                            one captured CUDA graph per cycle */
+  int32_t keep;         /* 1: keep the solve's device state (Krylov vectors, workspaces, captured
+                           graphs) with the operator for the next call with the same operators,
+                           nrhs and structure (freed with the operator) */
 } gila_solve_opts;
 
 typedef struct {

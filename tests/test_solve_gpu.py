@@ -214,3 +214,20 @@ def test_cast_operator_matvec(sys_):
     assert rel_l2(y32, y64) < 1e-5
     back = gila.cast(g32, np.complex128)
     assert rel_l2(back * x, y64) < 1e-6
+
+
+def test_keep_reuses_the_batch(sys_):
+    """keep=True: the second call reuses the resident batch and gives the
+    same field; a different nrhs or precision builds a new one."""
+    gila, G, ls, mem, chi, A = sys_
+    b = seeded_current(CEL, 50)
+    x0, i0 = gila.solve(ls, b, tol=TOL, mixed=True)
+    x1, i1 = gila.solve(ls, b, tol=TOL, mixed=True, keep=True)
+    x2, i2 = gila.solve(ls, b, tol=TOL, mixed=True, keep=True)
+    assert np.array_equal(x0, x1) and np.array_equal(x1, x2)
+    assert i1.iters == i2.iters == i0.iters and i2.outer == i1.outer
+    B = np.asfortranarray(np.stack([b, b], axis=-1))
+    X, _ = gila.solve(ls, B, tol=TOL, mixed=True, keep=True)
+    assert np.array_equal(X[..., 1], x0)
+    xp, _ = gila.solve(ls, b, tol=TOL, keep=True)
+    assert _res(A, xp, b) <= TOL
