@@ -192,6 +192,9 @@ def main():
     ap.add_argument("--no-sweep", action="store_true")
     ap.add_argument("--no-solve", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
+    ap.add_argument("--dtype", default="c128", choices=["c128", "c64"],
+                    help="precision of the main matvec workload (c64: ComplexF32, for profiling)")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the Poisson stream and of the burst that measures saturation")
     a = ap.parse_args()
@@ -214,7 +217,9 @@ def main():
     gila = load_pkg()
     gila.default_context(local)
 
-    mem, tru = make_opr(gila, CEL, np.complex128)
+    f32 = a.dtype == "c64"
+    ndt, tdt, cs = (np.complex64, torch.complex64, 8) if f32 else (np.complex128, torch.complex128, 16)
+    mem, tru = make_opr(gila, CEL, ndt)
     mem.reserve(1)
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     stream = torch.cuda.Stream()
@@ -225,7 +230,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
-    ms, y_dev = device_rate(torch, mem, CEL, CEL, torch.complex128, a.steps, W, stream, flush)
+    ms, y_dev = device_rate(torch, mem, CEL, CEL, tdt, a.steps, W, stream, flush)
     clocks = clk.stop()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
@@ -234,7 +239,7 @@ def main():
     value = world * a.steps / (ms_max / 1e3)
 
     # ---- e2e: public API with pinned host buffers, copies inside the timed region
-    xh = torch.randn((3, CEL[2], CEL[1], CEL[0]), dtype=torch.complex128).pin_memory()
+    xh = torch.randn((3, CEL[2], CEL[1], CEL[0]), dtype=tdt).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
     sp = stream.cuda_stream
     for _ in range(W):
@@ -260,24 +265,28 @@ def main():
 
     # ---- roofline of the dominant kernel (z pass), timed live
     passes = mem.time_passes(1, reps=max(3, min(a.steps, 10)))
-    zb = zpass_bytes(CEL, CEL, tru, 16)
+    zb = zpass_bytes(CEL, CEL, tru, cs)
     peak, peak_kind = measured_peak()
     achieved = zb / (passes[1] / 1e3) / 1e9
-    traffic = ncu_traffic("z_pass_c128_128x128x64")
-    roofline = {"bound": "hbm", "kernel": "k_z_ct (z pencils: FFT, 3x3 multiply, inverse FFT)",
+    traffic = ncu_traffic(f"z_pass_{a.dtype}_128x128x64")
+    roofline = {"bound": "hbm",
+                "kernel": ("k_zf2_ct" if f32 else "k_zf_ct") + " (z pencils: forward FFT, 3x3 multiply fused with "
+                          "the last / first butterflies, inverse FFT)",
                 "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "algorithmic_bytes_per_launch": zb, "launch_ms": round(passes[1], 4),
                 "pass_ms": {"xy_fwd": round(passes[0], 4), "z": round(passes[1], 4), "yx_inv": round(passes[2], 4)},
-                "matvec_tmin_bytes": tmin_bytes(CEL, CEL, tru, 16),
-                "matvec_tmin_frac": round(tmin_bytes(CEL, CEL, tru, 16) / (ms_max / a.steps / 1e3) / 1e9 / peak, 4)}
+                "matvec_tmin_bytes": tmin_bytes(CEL, CEL, tru, cs),
+                "matvec_tmin_frac": round(tmin_bytes(CEL, CEL, tru, cs) / (ms_max / a.steps / 1e3) / 1e9 / peak, 4)}
 
     out = {
-        "metric": METRIC, "value": round(value, 2), "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
+        "metric": METRIC if not f32 else METRIC.replace("ComplexF64", "ComplexF32"), "value": round(value, 2),
+        "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
         "warmup": W, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "complex128 (f64)",
+        "vs_baseline": None, "dtype": "complex64 (f32)" if f32 else "complex128 (f64)",
         "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
-        "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, ComplexF64, 1 vector/step",
+        "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
+                               + ("ComplexF32" if f32 else "ComplexF64") + ", 1 vector/step",
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
         "e2e": {"value": round(e2e_value, 2), "unit": "matvec/s", "h2d_bytes_per_step": nbytes,
                 "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors"},
@@ -286,7 +295,7 @@ def main():
         "clocks": clocks,
     }
 
-    if rank == 0 and world == 1:
+    if rank == 0 and world == 1 and not a.no_cpu:
         out["cpu_baseline"] = cpu_baseline()
     if not a.no_sweep and world == 1:
         out["sweep"] = sweep(torch, gila, stream, flush, y_dev)
@@ -590,7 +599,8 @@ def run_reference(a, world):
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / k * 1e3, 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
            "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel",
-           "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, ComplexF64, 1 vector/step",
+           "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
+                               + ("ComplexF32" if f32 else "ComplexF64") + ", 1 vector/step",
                       "parallelism": "host threads"},
            "cpu_baseline": {"value": round(val, 4), "unit": "matvec/s", "cores": n, "kind": "port", "sample": sample},
            "e2e": {"value": round(val, 4), "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
