@@ -193,4 +193,63 @@ function LinearAlgebra.mul!(y::AbstractArray{T}, o::GlaOpr, x::AbstractArray{T},
     y
 end
 
+# ---- the scattering solve (examples/GilaOperators.jl:57-96) ---------------
+
+struct CSolveOpts         # gila_solve_opts
+    tol::Cdouble; ell::Int32; mixed::Int32; max_matvecs::Int32; max_restarts::Int32
+    delta::Cdouble; x0::Int32; no_graph::Int32; keep::Int32
+end
+
+struct CSolveInfo         # gila_solve_info
+    iters::Int32; outer::Int32; matvecs_f64::Int32; matvecs_f32::Int32
+    rel_res::Cdouble; converged::Int32; breakdowns::Int32
+end
+
+"""LippmannSchwinger(G, medium): x -> x - medium .* (G x) (examples/GilaOperators.jl:57-82)."""
+struct LippmannSchwinger
+    greens_op::GlaOpr
+    medium::Array{ComplexF64,3}
+    g32::Base.RefValue{Any}
+end
+function LippmannSchwinger(G::GlaOpr, medium::AbstractArray{<:Complex,3})
+    glaSze(G, 1)[1:3] == size(medium) ||
+        throw(DimensionMismatch("Green's operator and medium must have the same size."))
+    LippmannSchwinger(G, ComplexF64.(medium), Ref{Any}(nothing))
+end
+
+function Base.:*(ls::LippmannSchwinger, x::AbstractArray)
+    gx = reshape(ls.greens_op * x, glaSze(ls.greens_op, 1))
+    x - reshape(ls.medium .* gx, size(x))
+end
+LinearAlgebra.mul!(y::AbstractArray, ls::LippmannSchwinger, x::AbstractArray) = y .= ls * x
+
+function g32(ls::LippmannSchwinger)
+    if ls.g32[] === nothing
+        r = Ref{Ptr{Cvoid}}(C_NULL)
+        check(ccall((:gila_opr_cast, LIB), Cint, (Ptr{Cvoid}, Cint, Ref{Ptr{Cvoid}}),
+                    ls.greens_op.mem.h, GILA_C64, r))
+        m = ls.greens_op.mem
+        ls.g32[] = GlaOprMem{ComplexF32}(r[], m.cmpInf, m.trgVol, m.srcVol)
+    end
+    ls.g32[]
+end
+
+"""solve(ls, i) (examples/scattering_film.jl:58-61): BiCGStab(l) on the GPU,
+`i` of size (Nx,Ny,Nz,3) or (Nx,Ny,Nz,3,nrhs); mixed = ComplexF32 Krylov with
+FP64 reliable updates.  Returns the solution (same shape) and the info."""
+function solve(ls::LippmannSchwinger, i::AbstractArray{ComplexF64}; tol=1e-6, mixed=true, ell=2,
+               max_matvecs=4000, keep=false)
+    n = 3 * prod(glaSze(ls.greens_op, 1)[1:3])
+    nrhs = length(i) ÷ n
+    b = Array(i); x = similar(b)
+    opts = Ref(CSolveOpts(tol, ell, mixed, max_matvecs, 0, 0.1, 0, 0, keep))
+    info = Ref{CSolveInfo}()
+    G32 = mixed ? g32(ls).h : C_NULL
+    check(ccall((:gila_ls_solve, LIB), Cint,
+                (Ptr{Cvoid}, Ptr{Cvoid}, Ptr{ComplexF64}, Ptr{ComplexF64}, Ptr{ComplexF64}, Int64,
+                 Ref{CSolveOpts}, Ref{CSolveInfo}, Ptr{Cdouble}, Ptr{Cvoid}),
+                ls.greens_op.mem.h, G32, ls.medium, b, x, nrhs, opts, info, C_NULL, C_NULL))
+    x, info[]
+end
+
 end # module
