@@ -157,3 +157,61 @@ def test_golden_fixtures_gpu():
                                  setTyp=dtype)
             y = gila.egoOpr(mem, np.asfortranarray(d["x"].astype(dtype)))
             assert rel_l2(y, d["y"]) <= tol, (f, dtype)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+@pytest.mark.parametrize("cels", [((8, 8, 8), (4, 4, 4)), ((8, 4, 8), (4, 4, 4)), ((4, 8, 8), (4, 4, 4)),
+                                  ((64, 64, 64), (32, 32, 32))],
+                         ids=lambda c: f"{c[0]}<-{c[1]}")
+def test_target_partitions(dtype, cels):
+    """Mixed cell scales (src/glaMem.jl:190-216): a target grid finer than
+    the source splits into target partitions (genPrt / mrgPrt,
+    src/glaActSup.jl:4-68, 939-1004); egoOpr! takes a source-partition-sized
+    input and scatters each target partition back into the full target.
+    External operators store the full spectrum, so any seeded kernel values
+    exercise the same code paths."""
+    from oracle.gla_mem import Vol, mix_for, tru_inf
+    gila = load_pkg()
+    tcel, scel = cels
+    tscl = tuple(f"1/{64 if t == 2 * s else 32}" for t, s in zip(tcel, scel))
+    trg = Vol.make(tcel, tscl, ("12/32", 0, 0))
+    src = Vol.make(scel, SCL, (0, 0, 0))
+    trg, src, mix, is_self = mix_for(trg, src)
+    assert not is_self and np.prod(mix.trg_div) > 1
+    tru = tru_inf(trg, src, mix)
+    par_t = int(np.prod(mix.trg_div))
+    rng = np.random.default_rng(5)
+    fur = [np.asfortranarray(rng.standard_normal((*tru, 6, 1, par_t)) + 1j * rng.standard_normal((*tru, 6, 1, par_t)))
+           for _ in range(8)]
+    mem = gila.GlaOprMem(gila.GlaKerOpt(True), gila.GlaVol(tcel, tscl, ("12/32", 0, 0)), gila.GlaVol(scel, SCL),
+                         egoFur=[f.astype(dtype) for f in fur], setTyp=dtype)
+    x = np.asfortranarray(seeded_current(mix.src_cel, 9).astype(dtype))
+    y = gila.egoOpr(mem, x)
+    assert tuple(y.shape) == (*tcel, 3)
+    ref = ego_opr(OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur]), x.astype(np.complex128))
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    assert rel_l2(y, ref) <= tol
+
+
+def test_source_partitions_rejected():
+    """A source grid finer than the target (several source partitions):
+    egoOpr! checks the input against the partition size and then cannot
+    split it into partitions (src/glaAct.jl:37-49 with the reshape of
+    egoBrnHst!), so the reference errors; the library reports GILA_ERR_SIZE."""
+    from oracle.gla_mem import Vol, mix_for, tru_inf
+    gila = load_pkg()
+    tcel, scel = (4, 4, 4), (8, 8, 8)
+    sscl = ("1/64", "1/64", "1/64")
+    trg, src, mix, _ = mix_for(Vol.make(tcel, SCL, ("12/32", 0, 0)), Vol.make(scel, sscl, (0, 0, 0)))
+    par_s = int(np.prod(mix.src_div))
+    assert par_s > 1
+    tru = tru_inf(trg, src, mix)
+    rng = np.random.default_rng(6)
+    fur = [np.asfortranarray(rng.standard_normal((*tru, 6, par_s, 1)) + 0j) for _ in range(8)]
+    x = np.asfortranarray(seeded_current(mix.src_cel, 3))
+    with pytest.raises(ValueError):
+        ego_opr(OprMem(mix, fur), x)
+    mem = gila.GlaOprMem(gila.GlaKerOpt(True), gila.GlaVol(tcel, SCL, ("12/32", 0, 0)), gila.GlaVol(scel, sscl),
+                         egoFur=fur)
+    with pytest.raises(gila.GilaError):
+        gila.egoOpr(mem, x)
