@@ -25,7 +25,7 @@ import os
 import statistics
 import subprocess
 import sys
-import tempfile
+import threading
 import time
 
 import numpy as np
@@ -83,37 +83,68 @@ def zpass_bytes(src, trg, tru, csize):
 
 
 class Clocks:
-    """nvidia-smi sampler (200 ms) around the timed region."""
+    """nvidia-smi sampler (every 50 ms) around the timed region.  Each sample
+    is stamped on arrival by a reader thread; the report covers the samples
+    that arrived between begin() and end() plus one sampling interval, so a
+    timed region shorter than the interval still gets the samples that
+    bracket it ("in_region" says how many fell inside)."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    INTERVAL_MS = 50
 
     def __init__(self, index):
-        self.index = index
-        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.rows, self.t0, self.t1 = [], None, None
+        self.lock = threading.Lock()
         try:
             self.p = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                       "-i", str(index), "-lms", "200"], stdout=self.f, stderr=subprocess.DEVNULL)
+                                       "-i", str(index), "-lms", str(self.INTERVAL_MS)],
+                                      stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except Exception:
             self.p = None
+            return
+        self.th = threading.Thread(target=self._read, daemon=True)
+        self.th.start()
+        # the first sample can take a second to appear: start timing after it
+        deadline = time.monotonic() + 5.0
+        while time.monotonic() < deadline:
+            with self.lock:
+                if self.rows:
+                    break
+            time.sleep(0.01)
+
+    def _read(self):
+        for line in self.p.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                with self.lock:
+                    self.rows.append((time.monotonic(), parts))
+
+    def begin(self):
+        self.t0 = time.monotonic()
+
+    def end(self):
+        self.t1 = time.monotonic()
 
     def stop(self):
         if self.p is None:
             return None
+        if self.t1 is None:
+            self.end()
+        # let the sample after the region arrive
+        time.sleep(1.5 * self.INTERVAL_MS / 1e3)
         self.p.terminate()
         try:
             self.p.wait(timeout=5)
         except Exception:
             self.p.kill()
-        self.f.flush()
-        rows = []
-        with open(self.f.name) as fh:
-            for line in fh:
-                parts = [x.strip() for x in line.split(",")]
-                if len(parts) >= 9:
-                    rows.append(parts)
-        os.unlink(self.f.name)
+        self.th.join(timeout=2)
+        t0 = self.t0 if self.t0 is not None else self.t1
+        pad = self.INTERVAL_MS / 1e3
+        with self.lock:
+            inside = [r for t, r in self.rows if t0 <= t <= self.t1]
+            rows = [r for t, r in self.rows if t0 - pad <= t <= self.t1 + pad]
         if not rows:
             return None
         sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
@@ -121,7 +152,8 @@ class Clocks:
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "in_region": len(inside),
+                "region_s": round(self.t1 - t0, 4), "interval_ms": self.INTERVAL_MS}
 
 
 def measured_peak():
@@ -161,7 +193,7 @@ def make_opr(gila, cel, dtype, seed=1, src_cel=None, trg_org=(0, 0, 0), src_org=
     return mem, tru
 
 
-def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, seed=3):
+def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, seed=3, clk=None):
     """matvec/s with device-resident vectors; per-step CUDA events, L2
     flushed between steps (outside the events)."""
     g = torch.Generator(device="cuda").manual_seed(seed)
@@ -172,6 +204,8 @@ def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, 
         mem.apply_into(x, y, stream=sp)
     torch.cuda.synchronize()
     ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
+    if clk:
+        clk.begin()
     with torch.cuda.stream(stream):
         for k in range(steps):
             flush.zero_()
@@ -179,6 +213,8 @@ def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, 
             mem.apply_into(x, y, stream=sp)
             ev[k][1].record(stream)
     torch.cuda.synchronize()
+    if clk:
+        clk.end()
     ms = sum(a.elapsed_time(b) for a, b in ev)
     return ms, y
 
@@ -186,7 +222,7 @@ def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-sweep", action="store_true")
@@ -230,7 +266,7 @@ def main():
         dist.barrier()
     torch.cuda.synchronize()
     clk = Clocks(local)
-    ms, y_dev = device_rate(torch, mem, CEL, CEL, tdt, a.steps, W, stream, flush)
+    ms, y_dev = device_rate(torch, mem, CEL, CEL, tdt, a.steps, W, stream, flush, clk=clk)
     clocks = clk.stop()
     t = torch.tensor([ms], dtype=torch.float64, device="cuda")
     if dist:
