@@ -853,6 +853,177 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
   }
 }
 
+// Two-stage fused z pass (FP64, P = 64 = 8 * 8).  The transform runs as two
+// radix-8 stages:
+//   A   forward, span 1: reads the source z planes of B straight into
+//       registers (all loads of a thread in flight at once), writes the
+//       shared tile;
+//   F   forward, span 8, the 3x3 multiply and the inverse's first stage on
+//       the same registers (as k_zf_ct), kernel values two frequencies ahead;
+//   B'  inverse, span 8: reads the shared tile, writes the target z planes.
+// Each element crosses shared memory twice instead of four times.  The same
+// two-stage form at P = 128 and 256 (radix 16 / 32 outer stages) needs about
+// 168 registers per thread; the lower occupancy cost more than the shared
+// traffic saved (measured 2% and 14% slower than k_zf_ct), so only P = 64
+// uses it (4% faster).
+constexpr int zr_r1(int P) { return P / 8; }
+constexpr int zr_threads(int TX, int P) { return TX * zr_r1(P); }
+constexpr int zr_min_blocks(int T) { return 65536 / (T * 168) > 1 ? 65536 / (T * 168) : 1; }
+constexpr bool zr_ok(int CS, int P, int TX) {
+  return CS == 16 && P == 64 && zr_threads(TX, P) >= 32 && zr_threads(TX, P) <= 256 &&
+         3LL * TX * P * CS <= 100 * 1024;
+}
+
+template <typename C, int P, int TX>
+__global__ void __launch_bounds__(zr_threads(TX, P), zr_min_blocks(zr_threads(TX, P))) k_zr_ct(const ZParams<C> p) {
+  using Tr = typename Real<C>::T;
+  constexpr int R2 = 8, R1 = zr_r1(P);
+  constexpr int T = TX * R1;
+  constexpr int CH = P * TX;
+  constexpr int NA = 3 * TX * R2;  // tasks of stages A and B': (component, line, j < R2)
+  constexpr int KA = (NA + T - 1) / T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nrhs = p.nrhs, ntiles = p.ntiles, Px = p.Px, Py = p.Py;
+  const int nin = p.nin, nout = p.nout;
+  const int rhs = blockIdx.x % nrhs;
+  const int rest = blockIdx.x / nrhs;
+  const int tseq = rest % ntiles;
+  const int yseq = rest / ntiles;
+  const int kx0 = tile_seq(tseq, ntiles) * TX;
+  const int ky = mirror_seq(yseq, Py);
+  const int tmax = Px - kx0;
+  const int64_t plane = (int64_t)Py * Px;
+  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
+  const C* const tw = p.tw;
+  // A: task (c, l, j) reads z = j + r * R2, r < R1 (zero past the source);
+  // output natural index j * R1 + r.  All tasks' loads go out first.
+  {
+    C v[KA][R1];
+#pragma unroll
+    for (int k = 0; k < KA; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      const int l = task % TX, q = task / TX, j = q % R2, c = q / R2;
+      const bool ok = (NA % T == 0 || task < NA) && l < tmax;
+      const C* const src = Bb + (int64_t)c * nin * plane + l;
+#pragma unroll
+      for (int r = 0; r < R1; ++r) {
+        const int i = j + r * R2;
+        v[k][r] = (ok && i < nin) ? __ldcs(src + (int64_t)i * plane) : czero<C>();
+      }
+    }
+#pragma unroll
+    for (int k = 0; k < KA; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NA % T == 0 || task < NA) {
+        const int l = task % TX, q = task / TX, j = q % R2, c = q / R2;
+        Bfly<R1, false, C>::run(v[k], tw, 0);
+        C* const dst = sm + c * CH + (j * R1) * TX + l;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) dst[r * TX] = v[k][r];
+      }
+    }
+  }
+  int py, iy, ry;
+  ax_map(p.ax[1], ky, py, iy, ry);
+  const int tx = p.tx, ty = p.ty, tz = p.tz;
+  const Tr s = (Tr)p.scale;
+  // F: task (l, j), j < R1: frequencies kz = j + r * R1
+  const int l = (int)threadIdx.x % TX, j = (int)threadIdx.x / TX;
+  int px, ix, rx;
+  ax_map(p.ax[0], kx0 + l, px, ix, rx);
+  auto kload = [&](int r, C* dst, int& rzo) {
+    int pz, iz;
+    ax_map(p.ax[2], j + r * R1, pz, iz, rzo);
+    const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) dst[q] = ker_ld(gp, q, tx);
+  };
+  // kernel values: two frequencies in flight (48 values for all eight do
+  // not fit); the first two go out before the barrier, under the forward
+  // stage
+  C ga[6], gb[6];
+  int rza = 0, rzb = 0;
+  if (l < tmax) {
+    kload(0, ga, rza);
+    kload(1, gb, rzb);
+  }
+  __syncthreads();
+  {
+    if (l < tmax) {
+      C v[3][R2];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < R2; ++r) v[c][r] = sm[c * CH + (j + r * R1) * TX + l];
+      {
+        C w[R2];
+        twiddles<R2, false>(tw, j, w);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int r = 1; r < R2; ++r) v[c][r] = cmul(v[c][r], w[r]);
+          Bfly<R2, false, C>::run(v[c], tw, R1);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < R2; ++r) {
+        C* const g = (r & 1) ? gb : ga;
+        const int rz = (r & 1) ? rzb : rza;
+        const C gxx = g[0], gyy = g[1], gzz = g[2];
+        const C gxy = cscale(g[3], (rx ^ ry) ? (Tr)-1 : (Tr)1);
+        const C gxz = cscale(g[4], (rx ^ rz) ? (Tr)-1 : (Tr)1);
+        const C gyz = cscale(g[5], (ry ^ rz) ? (Tr)-1 : (Tr)1);
+        const C x0 = v[0][r], x1 = v[1][r], x2 = v[2][r];
+        v[0][r] = cscale(cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2)), s);
+        v[1][r] = cscale(cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2)), s);
+        v[2][r] = cscale(cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2)), s);
+        // refill the set just used with frequency r + 2
+        asm volatile("" ::: "memory");
+        if (r + 2 < R2) {
+          if (r & 1)
+            kload(r + 2, gb, rzb);
+          else
+            kload(r + 2, ga, rza);
+        }
+      }
+      // inverse radix 8 (span 1): output natural index j * R2 + r goes back
+      // to the slot read, j + r * R1
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Bfly<R2, true, C>::run(v[c], tw, R1);
+#pragma unroll
+        for (int r = 0; r < R2; ++r) sm[c * CH + (j + r * R1) * TX + l] = v[c][r];
+      }
+    }
+  }
+  __syncthreads();
+  // B': task (c, l, j), j < R2, reads natural indices j + r * R2, which sit
+  // in slots j * R1 + r; twiddles w^(-r j); output z = j + r * R2
+#pragma unroll 1
+  for (int k = 0; k < KA; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NA % T == 0 || task < NA) {
+      const int l = task % TX, q = task / TX, j = q % R2, c = q / R2;
+      const C* const srcs = sm + c * CH + (j * R1) * TX + l;
+      C v[R1];
+#pragma unroll
+      for (int r = 0; r < R1; ++r) v[r] = srcs[r * TX];
+#pragma unroll
+      for (int r = 1; r < R1; ++r) v[r] = cmul(v[r], twid<true>(tw, r * j));
+      Bfly<R1, true, C>::run(v, tw, 0);
+      if (l < tmax) {
+        C* const Bo = Bb + (int64_t)c * nout * plane + l;
+#pragma unroll
+        for (int r = 0; r < R1; ++r) {
+          const int i = j + r * R2;
+          if (i < nout) Bo[(int64_t)i * plane] = v[r];
+        }
+      }
+    }
+  }
+}
+
 // The fused z pass for FP32 on line pairs (ct_stage2): same arithmetic as
 // k_zf_ct, each task moving two adjacent kx lines per shared-memory access.
 #ifndef GILA_ZF2_CAP
@@ -1073,6 +1244,14 @@ static inline bool zfuse() {
   }();
   return on;
 }
+// two-stage FP64 z pass (k_zr_ct) where it applies (GILA_ZTWO=0: k_zf_ct)
+static inline bool ztwo() {
+  static const bool on = [] {
+    const char* e = getenv("GILA_ZTWO");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 static inline bool zpair() {
   static const bool on = [] {
     const char* e = getenv("GILA_ZPAIR");
@@ -1289,6 +1468,15 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
 #define GILA_CT_Z2(n, tx)                             \
   if constexpr (ct_z_ok(sizeof(C), n, tx)) {          \
     if (p.P == n && p.TX == tx) {                     \
+      if constexpr (zr_ok(sizeof(C), n, tx)) {        \
+        if (p.parT == 1 && zfuse() && ztwo()) {       \
+          const void* fnr = (const void*)k_zr_ct<C, n, tx>; \
+          cudaError_t er = set_smem(fnr, sm);         \
+          if (er != cudaSuccess) return er;           \
+          k_zr_ct<C, n, tx><<<(unsigned)blocks, zr_threads(tx, n), sm, st>>>(p); \
+          return cudaGetLastError();                  \
+        }                                             \
+      }                                               \
       if constexpr (zf_ok(sizeof(C), n)) {            \
         if (p.parT == 1 && zfuse()) {                 \
           if constexpr (sizeof(C) == 8) {             \

@@ -27,6 +27,8 @@ CT_CASES = [
     ((16, 8, 192), None, (0, 0, 0)),        # z = 384
     ((16, 256, 8), None, (0, 0, 0)),        # y = 512
     ((64, 64, 32), (64, 64, 64), ("80/32", 0, 0)),  # external: 128, 128, 96
+    ((16, 8, 128), None, (0, 0, 0)),        # z = 256
+    ((16, 16, 48), (16, 16, 80), (0, 0, "100/32")),  # external z = 128, 80 source planes
 ]
 
 
