@@ -214,6 +214,14 @@ Core::~Core() {
   cudaFree(B);
   cudaFree(stage_in);
   cudaFree(stage_out);
+  for (cudaStream_t x : {st_h2d, st_d2h})
+    if (x) {
+      cudaStreamSynchronize(x);
+      cudaStreamDestroy(x);
+    }
+  for (int k = 0; k < 2; ++k)
+    for (cudaEvent_t x : {ev_in_ready[k], ev_in_free[k], ev_out_ready[k], ev_out_free[k]})
+      if (x) cudaEventDestroy(x);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -601,48 +609,106 @@ gila_status ensure_tuned(Core& c, int64_t nrhs) {
   return autotune(c, nrhs);
 }
 
+// staging buffer of at least n elements (contents not kept)
+static gila_status ensure_stage(void*& buf, int64_t& cap, int64_t n, size_t cs) {
+  if (cap >= n) return GILA_OK;
+  cudaFree(buf);
+  buf = nullptr;
+  cap = 0;
+  GILA_CUDA_TRY(cudaMalloc(&buf, (size_t)n * cs));
+  cap = n;
+  return GILA_OK;
+}
+
+// Several vectors in host memory: one vector at a time, the upload of vector
+// k + 1 and the download of vector k - 1 overlapping the passes of vector k
+// (upload, compute and download streams; two staging slots per direction,
+// events order each slot's reuse).  With pinned host memory the copies run
+// on the copy engines in both directions at once; pageable memory still
+// gives the right result, without the overlap.
+template <typename C>
+static gila_status apply_host_pipe(Core& c, const C* in, C* out, int64_t nrhs, bool din, bool dout, bool axpby, C a,
+                                   C b, cudaStream_t st) {
+  const int64_t ni = in_elems(c), no = out_elems(c);
+  const size_t cs = sizeof(C);
+  gila_status s;
+  if ((s = ensure_work(c, 1)) != GILA_OK) return s;
+  if ((s = ensure_tuned(c, 1)) != GILA_OK) return s;
+  if (!din && (s = ensure_stage(c.stage_in, c.stage_cap_in, 2 * ni, cs)) != GILA_OK) return s;
+  if (!dout && (s = ensure_stage(c.stage_out, c.stage_cap_out, 2 * no, cs)) != GILA_OK) return s;
+  for (cudaStream_t* x : {&c.st_h2d, &c.st_d2h})
+    if (!*x) GILA_CUDA_TRY(cudaStreamCreateWithFlags(x, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k)
+    for (cudaEvent_t* x : {&c.ev_in_ready[k], &c.ev_in_free[k], &c.ev_out_ready[k], &c.ev_out_free[k]})
+      if (!*x) GILA_CUDA_TRY(cudaEventCreateWithFlags(x, cudaEventDisableTiming));
+  const DevOp<C> d = devop<C>(c);
+  for (int64_t k = 0; k < nrhs; ++k) {
+    const int sl = (int)(k & 1);
+    const C* d_in = din ? in + k * ni : static_cast<const C*>(c.stage_in) + sl * ni;
+    C* d_out = dout ? out + k * no : static_cast<C*>(c.stage_out) + sl * no;
+    const bool up_out = !dout && axpby;  // beta * out needs the old values
+    if (!din || up_out) {
+      // the slots' previous vectors (k - 2) have been read by their passes
+      // and downloaded
+      GILA_CUDA_TRY(cudaStreamWaitEvent(c.st_h2d, c.ev_in_free[sl], 0));
+      if (up_out) GILA_CUDA_TRY(cudaStreamWaitEvent(c.st_h2d, c.ev_out_free[sl], 0));
+      if (!din)
+        GILA_CUDA_TRY(cudaMemcpyAsync(const_cast<C*>(d_in), in + k * ni, (size_t)ni * cs, cudaMemcpyHostToDevice,
+                                      c.st_h2d));
+      if (up_out)
+        GILA_CUDA_TRY(cudaMemcpyAsync(d_out, out + k * no, (size_t)no * cs, cudaMemcpyHostToDevice, c.st_h2d));
+      GILA_CUDA_TRY(cudaEventRecord(c.ev_in_ready[sl], c.st_h2d));
+      GILA_CUDA_TRY(cudaStreamWaitEvent(st, c.ev_in_ready[sl], 0));
+    }
+    if (!dout) GILA_CUDA_TRY(cudaStreamWaitEvent(st, c.ev_out_free[sl], 0));
+    GILA_CUDA_TRY(launch_matvec<C>(c.geom, d, c.launch, d_in, d_out, static_cast<C*>(c.A), static_cast<C*>(c.B), 1,
+                                   axpby, a, b, st));
+    GILA_CUDA_TRY(cudaEventRecord(c.ev_in_free[sl], st));
+    if (!dout) {
+      GILA_CUDA_TRY(cudaEventRecord(c.ev_out_ready[sl], st));
+      GILA_CUDA_TRY(cudaStreamWaitEvent(c.st_d2h, c.ev_out_ready[sl], 0));
+      GILA_CUDA_TRY(cudaMemcpyAsync(out + k * no, d_out, (size_t)no * cs, cudaMemcpyDeviceToHost, c.st_d2h));
+      GILA_CUDA_TRY(cudaEventRecord(c.ev_out_free[sl], c.st_d2h));
+    }
+  }
+  GILA_CUDA_TRY(cudaStreamSynchronize(st));
+  GILA_CUDA_TRY(cudaStreamSynchronize(c.st_d2h));
+  GILA_CUDA_TRY(cudaStreamSynchronize(c.st_h2d));
+  return GILA_OK;
+}
+
 template <typename C>
 static gila_status apply_t(Core& c, const void* in, void* out, int64_t nrhs, bool axpby, const double* alpha,
                            const double* beta, cudaStream_t user_st) {
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
   const size_t cs = sizeof(C);
-  gila_status s = ensure_work(c, nrhs);
-  if (s != GILA_OK) return s;
-  if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
   cudaStream_t st = user_st ? user_st : c.stream;
   const bool din = is_device_ptr(in), dout = is_device_ptr(out);
   // element alignment (the passes copy with 16 / 8 byte cp.async)
   if ((din && ((uintptr_t)in % cs)) || (dout && ((uintptr_t)out % cs)))
     return fail(GILA_ERR_ARG, "device vectors must be aligned to their complex element size");
-  const C* d_in = static_cast<const C*>(in);
-  C* d_out = static_cast<C*>(out);
-  if (!din) {
-    if (c.stage_cap_in < ni) {
-      cudaFree(c.stage_in);
-      c.stage_in = nullptr;
-      c.stage_cap_in = 0;
-      GILA_CUDA_TRY(cudaMalloc(&c.stage_in, (size_t)ni * cs));
-      c.stage_cap_in = ni;
-    }
-    GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_in, in, (size_t)ni * cs, cudaMemcpyHostToDevice, st));
-    d_in = static_cast<const C*>(c.stage_in);
-  }
-  if (!dout) {
-    if (c.stage_cap_out < no) {
-      cudaFree(c.stage_out);
-      c.stage_out = nullptr;
-      c.stage_cap_out = 0;
-      GILA_CUDA_TRY(cudaMalloc(&c.stage_out, (size_t)no * cs));
-      c.stage_cap_out = no;
-    }
-    if (axpby) GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_out, out, (size_t)no * cs, cudaMemcpyHostToDevice, st));
-    d_out = static_cast<C*>(c.stage_out);
-  }
   C a, b;
   a.x = alpha ? (decltype(a.x))alpha[0] : 1;
   a.y = alpha ? (decltype(a.y))alpha[1] : 0;
   b.x = beta ? (decltype(b.x))beta[0] : 0;
   b.y = beta ? (decltype(b.y))beta[1] : 0;
+  if ((!din || !dout) && nrhs > 1)
+    return apply_host_pipe<C>(c, static_cast<const C*>(in), static_cast<C*>(out), nrhs, din, dout, axpby, a, b, st);
+  gila_status s = ensure_work(c, nrhs);
+  if (s != GILA_OK) return s;
+  if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
+  const C* d_in = static_cast<const C*>(in);
+  C* d_out = static_cast<C*>(out);
+  if (!din) {
+    if ((s = ensure_stage(c.stage_in, c.stage_cap_in, ni, cs)) != GILA_OK) return s;
+    GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_in, in, (size_t)ni * cs, cudaMemcpyHostToDevice, st));
+    d_in = static_cast<const C*>(c.stage_in);
+  }
+  if (!dout) {
+    if ((s = ensure_stage(c.stage_out, c.stage_cap_out, no, cs)) != GILA_OK) return s;
+    if (axpby) GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_out, out, (size_t)no * cs, cudaMemcpyHostToDevice, st));
+    d_out = static_cast<C*>(c.stage_out);
+  }
   GILA_CUDA_TRY(launch_matvec<C>(c.geom, devop<C>(c), c.launch, d_in, d_out, static_cast<C*>(c.A),
                                  static_cast<C*>(c.B), (int)nrhs, axpby, a, b, st));
   if (!dout) GILA_CUDA_TRY(cudaMemcpyAsync(out, c.stage_out, (size_t)no * cs, cudaMemcpyDeviceToHost, st));

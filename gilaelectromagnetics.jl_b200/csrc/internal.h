@@ -74,6 +74,12 @@ struct Core {
   void* stage_in = nullptr;
   void* stage_out = nullptr;
   int64_t stage_cap_in = 0, stage_cap_out = 0;
+  // host-vector pipeline (several vectors in host memory): two staging
+  // slots per direction (in stage_in / stage_out), upload and download
+  // streams, per-slot events
+  cudaStream_t st_h2d = nullptr, st_d2h = nullptr;
+  cudaEvent_t ev_in_ready[2] = {nullptr, nullptr}, ev_in_free[2] = {nullptr, nullptr};
+  cudaEvent_t ev_out_ready[2] = {nullptr, nullptr}, ev_out_free[2] = {nullptr, nullptr};
   Launch launch{};
   bool tuned = false;
   cudaStream_t stream = nullptr;

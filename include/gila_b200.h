@@ -134,7 +134,11 @@ gila_status gila_opr_info(const gila_opr* opr, gila_dtype* dtype, int32_t* flags
  * counts (complex) of the buffers and are checked against the operator's
  * input and output sizes times nrhs (GILA_ERR_SIZE, as egoOpr!'s error).
  * `dtype` must match the operator (GILA_ERR_TYPE, as the eltype assertion of
- * src/glaLinAlg.jl:35). */
+ * src/glaLinAlg.jl:35).  Vectors may be in device or host memory; the call
+ * returns when a host `out` holds the result.  With nrhs > 1 and a vector in
+ * host memory the vectors go through the device one at a time, the upload of
+ * the next and the download of the previous overlapping the passes of the
+ * current one (pinned host memory lets both copy directions run at once). */
 gila_status gila_opr_apply(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len,
                            void* out, int64_t out_len, int64_t nrhs, void* stream);
 

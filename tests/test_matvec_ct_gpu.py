@@ -29,6 +29,14 @@ CT_CASES = [
     ((64, 64, 32), (64, 64, 64), ("80/32", 0, 0)),  # external: 128, 128, 96
     ((16, 8, 128), None, (0, 0, 0)),        # z = 256
     ((16, 16, 48), (16, 16, 80), (0, 0, "100/32")),  # external z = 128, 80 source planes
+    # equal x and y lengths: the fused x / y cluster pass
+    ((32, 32, 16), None, (0, 0, 0)),        # 64, 64
+    ((48, 48, 8), None, (0, 0, 0)),         # 96, 96
+    ((96, 96, 8), None, (0, 0, 0)),         # 192, 192
+    ((128, 128, 8), None, (0, 0, 0)),       # 256, 256
+    ((192, 192, 4), None, (0, 0, 0)),       # 384, 384
+    ((256, 256, 4), None, (0, 0, 0)),       # 512, 512
+    ((40, 64, 8), (24, 64, 8), ("50/32", 0, 0)),  # external 64, 128 ... x != y
 ]
 
 
@@ -66,10 +74,11 @@ def test_ct_matvec_parity_all_tiles(case, dtype):
         assert np.array_equal(y, outs[0])
 
 
+@pytest.mark.parametrize("case", [CT_CASES[1], ((64, 64, 8), None, (0, 0, 0))], ids=["xy-separate", "xy-fused"])
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
-def test_ct_multi_rhs(dtype):
+def test_ct_multi_rhs(dtype, case):
     gila = load_pkg()
-    mix, mem, ref = _build(gila, CT_CASES[1], dtype)
+    mix, mem, ref = _build(gila, case, dtype)
     xs = [np.asfortranarray(seeded_current(mix.src_cel, 20 + k).astype(dtype)) for k in range(3)]
     X = np.asfortranarray(np.stack(xs, axis=-1))
     Y = mem.new_output(X[..., 0], nrhs=3)

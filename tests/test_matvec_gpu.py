@@ -81,6 +81,54 @@ def test_multi_rhs_and_axpby(dtype):
     assert rel_l2(out, ref) <= tol
 
 
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_host_batches_pipelined(dtype):
+    """Several vectors in host memory go through the device one at a time
+    with overlapped copies: the same values as the batched device call,
+    for pinned and pageable host memory, host input or host output only,
+    and the fused axpby (whose old host output is uploaded per vector)."""
+    import torch
+    gila = load_pkg()
+    mix, fur, mem = _build(gila, ((64, 64, 8), None, (0, 0, 0), None), dtype)
+    n = 4
+    tdt = torch.complex128 if dtype == np.complex128 else torch.complex64
+    xs = [np.asfortranarray(seeded_current(mix.src_cel, 200 + k).astype(dtype)) for k in range(n)]
+    X = np.asfortranarray(np.stack(xs, axis=-1))
+    Xt = torch.from_numpy(np.ascontiguousarray(X.transpose(4, 3, 2, 1, 0)))
+    Xd = Xt.cuda()
+    Yd = torch.empty_like(Xd)
+    mem.apply_into(Xd, Yd, nrhs=n)
+    ref = Yd.cpu()
+    Yp = torch.empty_like(Xt).pin_memory()
+    mem.apply_into(Xt.pin_memory(), Yp, nrhs=n)                 # pinned host -> pinned host
+    assert torch.equal(Yp, ref)
+    Yh = torch.empty_like(Xt)
+    mem.apply_into(Xt, Yh, nrhs=n)                              # pageable host
+    assert torch.equal(Yh, ref)
+    Ym = torch.empty_like(Xt).pin_memory()
+    mem.apply_into(Xd, Ym, nrhs=n)                              # device in, host out
+    assert torch.equal(Ym, ref)
+    Yd2 = torch.empty_like(Xd)
+    mem.apply_into(Xt.pin_memory(), Yd2, nrhs=n)                # host in, device out
+    assert torch.equal(Yd2.cpu(), ref)
+    # axpby with host output: out = a G x + b out
+    a, b = 0.5 - 2j, 1.5 + 0.25j
+    O0 = torch.from_numpy(np.ascontiguousarray(
+        np.stack([seeded_current(mix.trg_cel, 300 + k).astype(dtype) for k in range(n)], axis=-1)
+        .transpose(4, 3, 2, 1, 0)))
+    Od = O0.cuda()
+    mem.axpby_into(a, Xd, b, Od, nrhs=n)
+    Oh = O0.clone().pin_memory()
+    mem.axpby_into(a, Xt.pin_memory(), b, Oh, nrhs=n)
+    assert torch.equal(Oh, Od.cpu())
+    assert Yp.dtype == tdt
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    om = OprMem(mix, [f.astype(dtype).astype(np.complex128) for f in fur])
+    got = Yp.numpy().transpose(4, 3, 2, 1, 0)
+    for k in range(n):
+        assert rel_l2(got[..., k], ego_opr(om, xs[k].astype(np.complex128))) <= tol
+
+
 def test_device_tensors_and_determinism():
     import torch
     gila = load_pkg()
