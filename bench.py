@@ -39,7 +39,7 @@ METRIC = "Green matvec/s (ComplexF64 egoOpr!, self 128x128x64)"
 CEL = (128, 128, 64)
 SCL = ("1/32", "1/32", "1/32")
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-E2E_BATCH = 8  # host vectors per API call in the end-to-end leg
+E2E_BATCH = 20  # host vectors per API call in the end-to-end leg
 
 
 def load_pkg():
@@ -329,10 +329,10 @@ def main():
         "vs_baseline": None, "dtype": "complex64 (f32)" if f32 else "complex128 (f64)",
         "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
         "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
-                               + ("ComplexF32" if f32 else "ComplexF64") + ", 1 vector/step",
+                               + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
         "e2e": {"value": round(e2e_value, 2), "unit": "matvec/s", "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors, 8 vectors per call (copies overlap the passes)"},
+                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors, 20 vectors per call (copies overlap the passes)"},
         "gpu_launches": int(mem.launches_per_apply(1)) * a.steps,
         "roofline": roofline,
         "clocks": clocks,
@@ -643,7 +643,7 @@ def run_reference(a, world):
            "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
            "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel",
            "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
-                               + ("ComplexF32" if f32 else "ComplexF64") + ", 1 vector/step",
+                               + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
                       "parallelism": "host threads"},
            "cpu_baseline": {"value": round(val, 4), "unit": "matvec/s", "cores": n, "kind": "port", "sample": sample},
            "e2e": {"value": round(val, 4), "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

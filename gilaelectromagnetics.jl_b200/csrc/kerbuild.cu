@@ -1313,6 +1313,16 @@ struct Build {
   ~Build() {
     for (auto* b : keep) delete b;
   }
+  // frees the buffers allocated after `mark` (the stream is synchronised
+  // first: kernels in flight may still use them)
+  void release_from(size_t mark) {
+    if (keep.size() <= mark) return;
+    cudaStreamSynchronize(st);
+    while (keep.size() > mark) {
+      delete keep.back();
+      keep.pop_back();
+    }
+  }
   template <typename T>
   gila_status alloc(T** out, size_t n) {
     DBuf* b = new DBuf;
@@ -1512,13 +1522,134 @@ static gila_status fft3(Build& B, Z* crc_d, const int P[3]) {
 
 }  // namespace kb
 
+namespace kb {
+
+// The external circulant of one target / source volume pair
+// (genEgoCrcExt!, src/glaGen.jl:55-100) into crc_d [6][P...].
+static gila_status ext_circulant(Build& B, const HVol& t, const HVol& sv, const int P[3], Z* crc_d, int* err_d) {
+  gila_status s;
+  const int64_t vol = (int64_t)P[0] * P[1] * P[2];
+  Rat sl[3], su[3], tl[3], tu[3];
+  bool c1 = true, c2 = true;
+  int ovr = 0;
+  for (int d = 0; d < 3; ++d) {
+    const Rat hs = rdv(sv.scl[d], R(2)), ht = rdv(t.scl[d], R(2));
+    sl[d] = rsub(sv.start[d], hs);
+    su[d] = radd(sv.stop[d], hs);
+    tl[d] = rsub(t.start[d], ht);
+    tu[d] = radd(t.stop[d], ht);
+    c1 = c1 && rle(sl[d], tl[d]) && rle(tl[d], su[d]);
+    c2 = c2 && rle(sl[d], tu[d]) && rle(tu[d], su[d]);
+    ovr += (rlt(sl[d], tl[d]) && rlt(tl[d], su[d])) + (rlt(sl[d], tu[d]) && rlt(tu[d], su[d]));
+  }
+  const bool contact = c1 || c2;
+  if (contact && ovr > 0) return fail(GILA_ERR_OVERLAP, "Source and target volumes are overlapping.");
+  // grdSel tables over sepGrd(trg, src, 0) / sepGrd(trg, src, 1)
+  double* sep_d[3];
+  for (int d = 0; d < 3; ++d) {
+    Rat tstr = rsub(t.start[d], sv.start[d]), tstp = rsub(t.stop[d], sv.start[d]), tstep = t.grd[d];
+    if (rlt(tstp, tstr)) tstep = rmul(tstep, R(-1));
+    Rat sstr = rsub(t.start[d], sv.stop[d]), sstp = rsub(t.start[d], sv.start[d]), sstep = sv.grd[d];
+    if (rlt(sstp, sstr)) sstep = rmul(sstep, R(-1));
+    std::vector<double> sp(P[d], 0.0);
+    for (int64_t ind = 1; ind <= P[d]; ++ind) {
+      if (ind <= t.cel[d]) {
+        sp[ind - 1] = rd(radd(tstr, rmul(R(ind - 1), tstep)));
+      } else if (ind > t.cel[d] + 1) {
+        sp[ind - 1] = rd(radd(sstr, rmul(R(ind - 2 - t.cel[d]), sstep)));
+      }
+    }
+    if ((s = B.alloc(&sep_d[d], sp.size())) != GILA_OK) return s;
+    KB_TRY(cudaMemcpyAsync(sep_d[d], sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, B.st));
+  }
+  PairGeo G;
+  faces(t.scl, G.tf);
+  faces(sv.scl, G.sf);
+  srf_scales(t.scl, sv.scl, G.scale);
+  G.f = B.f;
+  PairGeo* g_d;
+  if ((s = B.alloc(&g_d, 1)) != GILA_OK) return s;
+  KB_TRY(cudaMemcpyAsync(g_d, &G, sizeof(G), cudaMemcpyHostToDevice, B.st));
+  FarParams fp{};
+  fp.mode = 1;
+  for (int d = 0; d < 3; ++d) {
+    fp.n[d] = P[d];
+    fp.sep[d] = sep_d[d];
+    fp.split[d] = (int)t.cel[d];
+    fp.touch[d] = contact ? CNT_TOL + (rd(t.scl[d]) + rd(sv.scl[d])) / 2.0 : -1.0;
+  }
+  fp.nitems = vol;
+  fp.out = crc_d;
+  fp.errflag = err_d;
+  if ((s = run_far(B, fp, g_d)) != GILA_OK) return s;
+  if (contact) {
+    // genCntVol (src/glaGen.jl:308-318) and its self circulant
+    int64_t cel[3];
+    Rat cs[3];
+    for (int d = 0; d < 3; ++d) {
+      cs[d] = rlt(t.scl[d], sv.scl[d]) ? t.scl[d] : sv.scl[d];
+      const Rat a = rdv(t.scl[d], cs[d]), b = rdv(sv.scl[d], cs[d]);
+      cel[d] = a.n / a.d + b.n / b.d;
+    }
+    Vol cv0;
+    for (int d = 0; d < 3; ++d) {
+      cv0.cel[d] = cel[d];
+      cv0.scl[d] = cs[d];
+      cv0.org[d] = R(0);
+      cv0.grd[d] = cs[d];
+    }
+    const HVol cv = hvol(cv0);
+    Z* ccnt;
+    if ((s = B.alloc(&ccnt, 6 * 8 * cel[0] * cel[1] * cel[2])) != GILA_OK) return s;
+    if ((s = self_circulant(B, cv, ccnt, err_d)) != GILA_OK) return s;
+    CntParams cp;
+    for (int d = 0; d < 3; ++d) {
+      cp.n[d] = P[d];
+      cp.split[d] = (int)t.cel[d];
+      cp.sep[d] = sep_d[d];
+      cp.touch[d] = fp.touch[d];
+      cp.cscl[d] = rd(cs[d]);
+      const Rat ss = rdv(sv.scl[d], cs[d]), ts = rdv(t.scl[d], cs[d]);
+      cp.sspan[d] = (int)(ss.n / ss.d);
+      cp.tspan[d] = (int)(ts.n / ts.d);
+      cp.cc[d] = (int)cel[d];
+    }
+    cp.ccnt = ccnt;
+    cp.out = crc_d;
+    k_contact<<<64, 128, 0, B.st>>>(cp);
+    KB_TRY(cudaGetLastError());
+  }
+  return GILA_OK;
+}
+
+// Partition `tp` (x fastest) of a volume whose cells sit on a grid `div`
+// times coarser than the pair's common grid (src/glaMemSup.jl:60-87): centre
+// (off - (div - 1) / 2) * scl + org, cell scale scl, grid step div * scl,
+// par_cel cells per axis.
+static HVol partition_vol(const Vol& v, const int div[3], const int par_cel[3], const int off[3]) {
+  Vol p;
+  for (int d = 0; d < 3; ++d) {
+    p.cel[d] = par_cel[d];
+    p.scl[d] = v.scl[d];
+    p.org[d] = radd(rmul(rsub(R(off[d]), R(div[d] - 1, 2)), v.scl[d]), v.org[d]);
+    p.grd[d] = rmul(R(div[d]), v.scl[d]);
+  }
+  return hvol(p);
+}
+
+}  // namespace kb
+
 // Build the operator's Fourier kernel on the GPU (GlaOprMem with
-// egoFur == nothing).  Single-partition operators only.
+// egoFur == nothing).  Volume pairs of different cell scales are built per
+// target partition (src/glaMemSup.jl:60-88), each partition's circulant
+// transformed and extracted into its slice of the kernel.  Source
+// partitions (a source grid finer than the target) are refused: egoOpr!
+// cannot apply such an operator (src/glaAct.jl:37-49).
 gila_status build_kernel(Core& c) {
   using namespace kb;
-  if (c.parS != 1 || c.geom.parT != 1)
-    return fail(GILA_ERR_ARG, "the GPU kernel build does not handle partitioned (mixed-scale) volumes; "
-                              "pass egoFur instead");
+  if (c.parS != 1)
+    return fail(GILA_ERR_ARG, "the GPU kernel build does not handle source partitions (a source grid finer than "
+                              "the target), which egoOpr! cannot apply; pass egoFur instead");
   Build B;
   B.ctx = c.ctx;
   B.st = c.stream;
@@ -1544,115 +1675,32 @@ gila_status build_kernel(Core& c) {
   const int64_t vol = (int64_t)P[0] * P[1] * P[2];
   Z* crc_d;
   if ((s = B.alloc(&crc_d, 6 * vol)) != GILA_OK) return s;
-  if (c.self) {
-    if ((s = self_circulant(B, t, crc_d, err_d)) != GILA_OK) return s;
-  } else {
-    // external circulant (genEgoCrcExt!, src/glaGen.jl:55-100)
-    Rat sl[3], su[3], tl[3], tu[3];
-    bool c1 = true, c2 = true;
-    int ovr = 0;
-    for (int d = 0; d < 3; ++d) {
-      const Rat hs = rdv(sv.scl[d], R(2)), ht = rdv(t.scl[d], R(2));
-      sl[d] = rsub(sv.start[d], hs);
-      su[d] = radd(sv.stop[d], hs);
-      tl[d] = rsub(t.start[d], ht);
-      tu[d] = radd(t.stop[d], ht);
-      c1 = c1 && rle(sl[d], tl[d]) && rle(tl[d], su[d]);
-      c2 = c2 && rle(sl[d], tu[d]) && rle(tu[d], su[d]);
-      ovr += (rlt(sl[d], tl[d]) && rlt(tl[d], su[d])) + (rlt(sl[d], tu[d]) && rlt(tu[d], su[d]));
-    }
-    const bool contact = c1 || c2;
-    if (contact && ovr > 0) return fail(GILA_ERR_OVERLAP, "Source and target volumes are overlapping.");
-    // grdSel tables over sepGrd(trg, src, 0) / sepGrd(trg, src, 1)
-    double* sep_d[3];
-    for (int d = 0; d < 3; ++d) {
-      Rat tstr = rsub(t.start[d], sv.start[d]), tstp = rsub(t.stop[d], sv.start[d]), tstep = t.grd[d];
-      if (rlt(tstp, tstr)) tstep = rmul(tstep, R(-1));
-      Rat sstr = rsub(t.start[d], sv.stop[d]), sstp = rsub(t.start[d], sv.start[d]), sstep = sv.grd[d];
-      if (rlt(sstp, sstr)) sstep = rmul(sstep, R(-1));
-      std::vector<double> sp(P[d], 0.0);
-      for (int64_t ind = 1; ind <= P[d]; ++ind) {
-        if (ind <= t.cel[d]) {
-          sp[ind - 1] = rd(radd(tstr, rmul(R(ind - 1), tstep)));
-        } else if (ind > t.cel[d] + 1) {
-          sp[ind - 1] = rd(radd(sstr, rmul(R(ind - 2 - t.cel[d]), sstep)));
-        }
-      }
-      if ((s = B.alloc(&sep_d[d], sp.size())) != GILA_OK) return s;
-      KB_TRY(cudaMemcpyAsync(sep_d[d], sp.data(), sp.size() * sizeof(double), cudaMemcpyHostToDevice, B.st));
-    }
-    PairGeo G;
-    faces(t.scl, G.tf);
-    faces(sv.scl, G.sf);
-    srf_scales(t.scl, sv.scl, G.scale);
-    G.f = B.f;
-    PairGeo* g_d;
-    if ((s = B.alloc(&g_d, 1)) != GILA_OK) return s;
-    KB_TRY(cudaMemcpyAsync(g_d, &G, sizeof(G), cudaMemcpyHostToDevice, B.st));
-    FarParams fp{};
-    fp.mode = 1;
-    for (int d = 0; d < 3; ++d) {
-      fp.n[d] = P[d];
-      fp.sep[d] = sep_d[d];
-      fp.split[d] = (int)t.cel[d];
-      fp.touch[d] = contact ? CNT_TOL + (rd(t.scl[d]) + rd(sv.scl[d])) / 2.0 : -1.0;
-    }
-    fp.nitems = vol;
-    fp.out = crc_d;
-    fp.errflag = err_d;
-    if ((s = run_far(B, fp, g_d)) != GILA_OK) return s;
-    if (contact) {
-      // genCntVol (src/glaGen.jl:308-318) and its self circulant
-      int64_t cel[3];
-      Rat cs[3];
-      for (int d = 0; d < 3; ++d) {
-        cs[d] = rlt(t.scl[d], sv.scl[d]) ? t.scl[d] : sv.scl[d];
-        const Rat a = rdv(t.scl[d], cs[d]), b = rdv(sv.scl[d], cs[d]);
-        cel[d] = a.n / a.d + b.n / b.d;
-      }
-      Vol cv0;
-      for (int d = 0; d < 3; ++d) {
-        cv0.cel[d] = cel[d];
-        cv0.scl[d] = cs[d];
-        cv0.org[d] = R(0);
-        cv0.grd[d] = cs[d];
-      }
-      const HVol cv = hvol(cv0);
-      Z* ccnt;
-      if ((s = B.alloc(&ccnt, 6 * 8 * cel[0] * cel[1] * cel[2])) != GILA_OK) return s;
-      if ((s = self_circulant(B, cv, ccnt, err_d)) != GILA_OK) return s;
-      CntParams cp;
-      for (int d = 0; d < 3; ++d) {
-        cp.n[d] = P[d];
-        cp.split[d] = (int)t.cel[d];
-        cp.sep[d] = sep_d[d];
-        cp.touch[d] = fp.touch[d];
-        cp.cscl[d] = rd(cs[d]);
-        const Rat ss = rdv(sv.scl[d], cs[d]), ts = rdv(t.scl[d], cs[d]);
-        cp.sspan[d] = (int)(ss.n / ss.d);
-        cp.tspan[d] = (int)(ts.n / ts.d);
-        cp.cc[d] = (int)cel[d];
-      }
-      cp.ccnt = ccnt;
-      cp.out = crc_d;
-      k_contact<<<64, 128, 0, B.st>>>(cp);
-      KB_TRY(cudaGetLastError());
-    }
-  }
-  if ((s = fft3(B, crc_d, P)) != GILA_OK) return s;
-  // extract into the operator's kernel layout
   const Geom& g = c.geom;
+  const int parT = g.parT;
   const size_t cs = csize(c.dtype);
-  const size_t bytes = (size_t)g.tru[0] * g.tru[1] * g.tru[2] * 6 * 8 * cs;
-  KB_TRY(cudaMalloc(&c.ker, bytes));
-  c.ker_bytes = bytes;
-  if (c.dtype == GILA_C128)
-    k_extract<double2><<<1184, 256, 0, B.st>>>(crc_d, P[0], P[1], P[2], g.tru[0], g.tru[1], g.tru[2],
-                                              static_cast<double2*>(c.ker), err_d + 1);
-  else
-    k_extract<float2><<<1184, 256, 0, B.st>>>(crc_d, P[0], P[1], P[2], g.tru[0], g.tru[1], g.tru[2],
-                                             static_cast<float2*>(c.ker), err_d + 1);
-  KB_TRY(cudaGetLastError());
+  const size_t per = (size_t)g.tru[0] * g.tru[1] * g.tru[2] * 6 * 8;  // elements per target partition
+  KB_TRY(cudaMalloc(&c.ker, per * parT * cs));
+  c.ker_bytes = per * parT * cs;
+  const size_t mark = B.keep.size();
+  for (int tp = 0; tp < parT; ++tp) {
+    if (c.self) {
+      if ((s = self_circulant(B, t, crc_d, err_d)) != GILA_OK) return s;
+    } else {
+      KB_TRY(cudaMemsetAsync(crc_d, 0, (size_t)6 * vol * sizeof(Z), B.st));
+      const HVol tv = parT == 1 ? t : partition_vol(c.trg, c.mix.tdiv, c.mix.tc, g.toff[tp]);
+      if ((s = ext_circulant(B, tv, sv, P, crc_d, err_d)) != GILA_OK) return s;
+    }
+    if ((s = fft3(B, crc_d, P)) != GILA_OK) return s;
+    // extract into partition tp of the operator's kernel layout
+    if (c.dtype == GILA_C128)
+      k_extract<double2><<<1184, 256, 0, B.st>>>(crc_d, P[0], P[1], P[2], g.tru[0], g.tru[1], g.tru[2],
+                                                static_cast<double2*>(c.ker) + per * tp, err_d + 1);
+    else
+      k_extract<float2><<<1184, 256, 0, B.st>>>(crc_d, P[0], P[1], P[2], g.tru[0], g.tru[1], g.tru[2],
+                                               static_cast<float2*>(c.ker) + per * tp, err_d + 1);
+    KB_TRY(cudaGetLastError());
+    B.release_from(mark);  // this partition's cubature scratch
+  }
   int flags[2];
   KB_TRY(cudaMemcpyAsync(flags, err_d, sizeof(flags), cudaMemcpyDeviceToHost, B.st));
   KB_TRY(cudaStreamSynchronize(B.st));

@@ -120,18 +120,53 @@ def ext_circulant(trg: Vol, src: Vol, frq=1.0 + 0j, int_ord=32):
     return _crc_to_rc(raw[0::2] + 1j * raw[1::2], P)
 
 
-def build_operator(trg_cel, scl, trg_org=(0, 0, 0), src_cel=None, src_org=None, frq=1.0 + 0j, int_ord=32,
-                   set_dtype=np.complex128, weak_vals=None):
-    """GlaOprMem without egoFur (src/glaMemSup.jl:16-171), single partition:
-    returns (mix, fur, crc, is_self, trg, src)."""
-    trg = Vol.make(trg_cel, scl, trg_org)
-    src = None if src_cel is None else Vol.make(src_cel, scl, src_org)
+def partition_vols(vol: Vol, div, par_cel):
+    """The partitions of a volume whose cells sit on a grid `div` times
+    coarser than the pair's common grid (src/glaMemSup.jl:60-87): partition
+    offsets x fastest, centre ((off - (div - 1) / 2) * scl + org), cell
+    scale scl, grid step div * scl."""
+    out = []
+    for k in range(div[2]):
+        for j in range(div[1]):
+            for i in range(div[0]):
+                off = (i, j, k)
+                org = tuple((Fraction(o) - Fraction(d - 1, 2)) * s + g
+                            for o, d, s, g in zip(off, div, vol.scl, vol.org))
+                grd = tuple(d * s for d, s in zip(div, vol.scl))
+                out.append(Vol(tuple(par_cel), vol.scl, org, grd))
+    return out
+
+
+def build_operator_vols(trg: Vol, src: Vol | None, frq=1.0 + 0j, int_ord=32, set_dtype=np.complex128,
+                        weak_vals=None):
+    """GlaOprMem without egoFur (src/glaMemSup.jl:16-171) for volume pairs of
+    any compatible scales: the external circulant of every (source,
+    target) partition pair, crc[3,3,P...,parS,parT], then the Fourier
+    kernel.  Returns (mix, fur, crc, is_self, trg, src)."""
     trg, src, mix, is_self = mix_for(trg, src)
     if is_self:
         crc = self_circulant(trg, frq, int_ord, weak_vals)
     else:
-        crc = ext_circulant(trg, src, frq, int_ord)
+        tp = partition_vols(trg, mix.trg_div, mix.trg_cel)
+        sp = partition_vols(src, mix.src_div, mix.src_cel)
+        if len(tp) * len(sp) == 1:
+            crc = ext_circulant(trg, src, frq, int_ord)
+        else:
+            P = [t + s for t, s in zip(mix.trg_cel, mix.src_cel)]
+            crc = np.empty((3, 3, *P, len(sp), len(tp)), dtype=np.complex128)
+            for ti, tv in enumerate(tp):
+                for si, sv in enumerate(sp):
+                    crc[..., si, ti] = ext_circulant(tv, sv, frq, int_ord)
     if not np.all(np.isfinite(crc)):
         raise ValueError("Computed circulant contains non-numeric values.")
     fur = crc_to_fur(crc, tru_inf(trg, src, mix), set_dtype)
     return mix, fur, crc, is_self, trg, src
+
+
+def build_operator(trg_cel, scl, trg_org=(0, 0, 0), src_cel=None, src_org=None, frq=1.0 + 0j, int_ord=32,
+                   set_dtype=np.complex128, weak_vals=None, src_scl=None):
+    """GlaOprMem without egoFur for a target (and source) given by cells,
+    scale and centre; `src_scl` defaults to the target's scale."""
+    trg = Vol.make(trg_cel, scl, trg_org)
+    src = None if src_cel is None else Vol.make(src_cel, scl if src_scl is None else src_scl, src_org)
+    return build_operator_vols(trg, src, frq, int_ord, set_dtype, weak_vals)

@@ -74,3 +74,47 @@ def test_gpu_build_complex64_and_overlap_error():
         assert np.abs(a.astype(np.complex64) - b).max() == 0  # cast of the same FP64 build
     with pytest.raises(gila.GilaError, match="overlapping"):
         gila.GlaOprMem(_opt(gila, 8), gila.GlaVol((4, 4, 4), scl, ("1/32", 0, 0)), gila.GlaVol((4, 4, 4), scl))
+
+
+PART_CASES = [
+    # (trg_cel, trg_scl, trg_org, src_cel): source at the origin, scale 1/32
+    ((8, 8, 8), ("1/64", "1/64", "1/64"), ("12/32", 0, 0), (4, 4, 4)),   # 8 target partitions
+    ((8, 4, 8), ("1/64", "1/32", "1/64"), (0, 0, "12/32"), (4, 4, 4)),   # 4, divided along x and z
+]
+
+
+@pytest.mark.parametrize("case", PART_CASES, ids=lambda c: f"{c[0]}@{c[1][0]}<-{c[3]}")
+def test_gpu_partitioned_build_matches_oracle(case):
+    """Mixed cell scales: the kernel of every target partition
+    (src/glaMemSup.jl:60-88) built on the GPU against the oracle's loop over
+    partition pairs, then the partitioned matvec on it."""
+    gila = load_pkg()
+    tc, tscl, to, sc = case
+    scl = ("1/32", "1/32", "1/32")
+    mix, fur_ref, _, is_self, trg, src = kb.build_operator(tc, tscl, to, sc, (0, 0, 0), int_ord=8, src_scl=scl)
+    assert not is_self and np.prod(mix.trg_div) > 1 and fur_ref[0].shape[5] == np.prod(mix.trg_div)
+    mem = gila.GlaOprMem(_opt(gila, 8), gila.GlaVol(trg.cel, trg.scl, trg.org), gila.GlaVol(src.cel, src.scl, src.org),
+                         setTyp=np.complex128)
+    fur = mem.egoFur
+    assert all(a.shape == b.shape for a, b in zip(fur, fur_ref))
+    scale = max(np.abs(f).max() for f in fur_ref)
+    err = max(np.abs(a - b).max() for a, b in zip(fur, fur_ref)) / scale
+    assert err < 1e-9, err
+    x = seeded_current(mix.src_cel, 6)
+    y = gila.egoOpr(mem, np.asfortranarray(x))
+    assert rel_l2(y, ego_opr(OprMem(mix, fur_ref), x)) < 1e-9
+
+
+def test_gpu_partitioned_build_errors():
+    """A partitioned target touching the source: each partition's cells lie
+    strictly inside the source's faces, which genEgoCrcExt! reports as an
+    overlap (src/glaGen.jl:66-80) -- on both sides.  A source grid finer
+    than the target (source partitions) is refused by the GPU build."""
+    gila = load_pkg()
+    scl = ("1/32", "1/32", "1/32")
+    with pytest.raises(ValueError, match="overlapping"):
+        kb.build_operator((8, 8, 8), ("1/64",) * 3, ("4/32", 0, 0), (4, 4, 4), (0, 0, 0), int_ord=8, src_scl=scl)
+    with pytest.raises(gila.GilaError, match="overlapping"):
+        gila.GlaOprMem(_opt(gila, 8), gila.GlaVol((8, 8, 8), ("1/64",) * 3, ("4/32", 0, 0)), gila.GlaVol((4, 4, 4), scl))
+    with pytest.raises(gila.GilaError, match="source partitions"):
+        gila.GlaOprMem(_opt(gila, 8), gila.GlaVol((4, 4, 4), scl, ("12/32", 0, 0)), gila.GlaVol((8, 8, 8), ("1/64",) * 3))
