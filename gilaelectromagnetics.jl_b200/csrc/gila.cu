@@ -642,6 +642,16 @@ static gila_status apply_host_pipe(Core& c, const C* in, C* out, int64_t nrhs, b
     for (cudaEvent_t* x : {&c.ev_in_ready[k], &c.ev_in_free[k], &c.ev_out_ready[k], &c.ev_out_free[k]})
       if (!*x) GILA_CUDA_TRY(cudaEventCreateWithFlags(x, cudaEventDisableTiming));
   const DevOp<C> d = devop<C>(c);
+  // every exit waits for the copies in flight: the caller may free or reuse
+  // its host buffers as soon as the call returns, on success or error
+  struct Drain {
+    cudaStream_t a, b, c;
+    ~Drain() {
+      cudaStreamSynchronize(a);
+      cudaStreamSynchronize(b);
+      cudaStreamSynchronize(c);
+    }
+  } drain{st, c.st_h2d, c.st_d2h};
   for (int64_t k = 0; k < nrhs; ++k) {
     const int sl = (int)(k & 1);
     const C* d_in = din ? in + k * ni : static_cast<const C*>(c.stage_in) + sl * ni;
@@ -674,7 +684,7 @@ static gila_status apply_host_pipe(Core& c, const C* in, C* out, int64_t nrhs, b
   GILA_CUDA_TRY(cudaStreamSynchronize(st));
   GILA_CUDA_TRY(cudaStreamSynchronize(c.st_d2h));
   GILA_CUDA_TRY(cudaStreamSynchronize(c.st_h2d));
-  return GILA_OK;
+  return GILA_OK;  // (the drain's waits are then no-ops)
 }
 
 template <typename C>
@@ -699,6 +709,14 @@ static gila_status apply_t(Core& c, const void* in, void* out, int64_t nrhs, boo
   if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
   const C* d_in = static_cast<const C*>(in);
   C* d_out = static_cast<C*>(out);
+  // host vectors: an error return also waits for the copies already queued
+  struct Drain {
+    cudaStream_t st;
+    bool on;
+    ~Drain() {
+      if (on) cudaStreamSynchronize(st);
+    }
+  } drain{st, !din || !dout};
   if (!din) {
     if ((s = ensure_stage(c.stage_in, c.stage_cap_in, ni, cs)) != GILA_OK) return s;
     GILA_CUDA_TRY(cudaMemcpyAsync(c.stage_in, in, (size_t)ni * cs, cudaMemcpyHostToDevice, st));
