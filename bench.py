@@ -232,6 +232,10 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--dtype", default="c128", choices=["c128", "c64"],
                     help="precision of the main matvec workload (c64: ComplexF32, for profiling)")
+    ap.add_argument("--profile", choices=["solve", "build"], default=None,
+                    help="run a small bounded workload for a profiler's launch list instead of the bench: "
+                         "'solve' = two short mixed-precision solves on 96x96x48, 'build' = the GPU kernel "
+                         "build of a 32^3 self operator; prints no bench line")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the Poisson stream and of the burst that measures saturation")
     a = ap.parse_args()
@@ -243,6 +247,8 @@ def main():
         if rank != 0:
             return 0
         return run_reference(a, world)
+    if a.profile:
+        return run_profile(a.profile)
 
     import torch
     torch.cuda.set_device(local)
@@ -326,7 +332,7 @@ def main():
         "metric": METRIC if not f32 else METRIC.replace("ComplexF64", "ComplexF32"), "value": round(value, 2),
         "unit": "matvec/s", "n_gpus": world, "steps": a.steps,
         "warmup": W, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "complex64 (f32)" if f32 else "complex128 (f64)",
+        "vs_baseline": None, "dtype": "f32" if f32 else "f64",
         "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
         "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
                                + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
@@ -339,7 +345,8 @@ def main():
     }
 
     if rank == 0 and world == 1 and not a.no_cpu:
-        out["cpu_baseline"] = cpu_baseline()
+        out["cpu_baseline"], xo, yo = cpu_baseline()
+        out["oracle_check"] = oracle_check(gila, xo, yo)
     if not a.no_sweep and world == 1:
         out["sweep"] = sweep(torch, gila, stream, flush, y_dev)
     if not a.no_solve and world == 1:
@@ -600,7 +607,7 @@ def cpu_baseline():
     rng = np.random.default_rng(3)
     x = rng.standard_normal((*CEL, 3)) + 1j * rng.standard_normal((*CEL, 3))
     om = OprMem(mix, fur)
-    ego_opr(om, x)  # warm-up
+    y = ego_opr(om, x)  # warm-up; its result checks the GPU matvecs
     reps = 2
     t0 = time.perf_counter()
     for _ in range(reps):
@@ -608,7 +615,51 @@ def cpu_baseline():
     dt = time.perf_counter() - t0
     return {"value": round(reps / dt, 4), "unit": "matvec/s", "cores": n, "kind": "port",
             "sample": f"{reps} matvecs of the same 128x128x64 ComplexF64 self operator (numpy/scipy.fft "
-                      f"restatement of egoBrnHst!, FFT workers={n}, elementwise steps single-threaded)"}
+                      f"restatement of egoBrnHst!, FFT workers={n}, elementwise steps single-threaded)"}, x, y
+
+
+def oracle_check(gila, x, y_ref):
+    """Relative L2 error of the GPU ComplexF64 and ComplexF32 matvecs of the
+    bench operator against the oracle's FP64 result on the same input (the
+    ComplexF32 operator holds the same kernel values rounded)."""
+    out = {}
+    xf = np.asfortranarray(x)
+    for dt, key in ((np.complex128, "rel_l2_f64"), (np.complex64, "rel_l2_f32")):
+        mem, _ = make_opr(gila, CEL, dt)
+        yg = np.asarray(gila.egoOpr(mem, xf.astype(dt))).astype(np.complex128)
+        out[key] = float(np.linalg.norm((yg - y_ref).ravel()) / np.linalg.norm(y_ref.ravel()))
+        del mem
+    out["tolerance"] = {"f64": 1e-12, "f32": 1e-5}
+    out["input"] = "seeded N(0,1) current (seed 3) through the bench operator; oracle: FP64 restatement of egoBrnHst!"
+    return out
+
+
+def run_profile(kind):
+    """Small bounded workloads whose every kernel a profiler's launch list
+    can cover: the Krylov-cycle kernels of the solver (two solves of 12
+    matvecs, ComplexF32 with FP64 reliable updates, on 96x96x48 with a slab
+    medium; the first one also sets up the batch and its graphs) or the GPU
+    kernel build (32^3 self operator, intOrd 16)."""
+    import torch
+    gila = load_pkg()
+    if kind == "build":
+        opt = gila.GlaKerOpt(1.0 + 0j, 16, False, True, (), ())
+        gila.GlaOprMem(opt, gila.GlaVol((32, 32, 32), SCL))
+        torch.cuda.synchronize()
+        return 0
+    cel = (96, 96, 48)
+    mem, _ = make_opr(gila, cel, np.complex128)
+    G = gila.GlaOpr(mem)
+    chi = np.zeros(cel, dtype=np.complex128, order="F")
+    chi[:, :, 12:36] = 3.0 + 0.1j
+    ls = gila.LippmannSchwinger(G, chi)
+    ls.g32()
+    b = torch.from_numpy(np.ascontiguousarray(plane_wave(cel).reshape(-1, order="F"))).cuda()
+    b = b.reshape(3, cel[2], cel[1], cel[0])
+    for _ in range(2):
+        gila.solve(ls, b, tol=1e-6, mixed=True, max_matvecs=12, check=False, keep=True)
+    torch.cuda.synchronize()
+    return 0
 
 
 def run_reference(a, world):
@@ -640,7 +691,7 @@ def run_reference(a, world):
               f"numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n}")
     out = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "matvec/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / k * 1e3, 2), "higher_is_better": True,
-           "scaling": "weak", "vs_baseline": None, "dtype": "complex128 (f64)",
+           "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.dtype == "c64" else "f64",
            "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel",
            "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
                                + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
