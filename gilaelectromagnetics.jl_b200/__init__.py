@@ -347,6 +347,18 @@ class GlaOprMem:
         t = (ct.c_int32 * 4)(*[int(a) for a in v])
         _check(L.lib().gila_opr_set_tiles(self._h, t))
 
+    @property
+    def schedule(self):
+        """Radix order of the x and y transforms: (x, y), 0 greedy, 1 reversed."""
+        t = (ct.c_int32 * 2)()
+        _check(L.lib().gila_opr_get_schedule(self._h, t))
+        return tuple(t)
+
+    @schedule.setter
+    def schedule(self, v):
+        t = (ct.c_int32 * 2)(*[int(a) for a in v])
+        _check(L.lib().gila_opr_set_schedule(self._h, t))
+
     def launches_per_apply(self, nrhs: int = 1) -> int:
         n = ct.c_int64()
         _check(L.lib().gila_opr_launches_per_apply(self._h, int(nrhs), ct.byref(n)))

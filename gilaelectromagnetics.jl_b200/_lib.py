@@ -104,6 +104,8 @@ _SIGS = [
     ("gila_opr_autotune", ct.c_int, [ct.c_void_p, ct.c_int64, ct.c_int32 * 4]),
     ("gila_opr_get_tiles", ct.c_int, [ct.c_void_p, ct.c_int32 * 4]),
     ("gila_opr_set_tiles", ct.c_int, [ct.c_void_p, ct.c_int32 * 4]),
+    ("gila_opr_get_schedule", ct.c_int, [ct.c_void_p, ct.c_int32 * 2]),
+    ("gila_opr_set_schedule", ct.c_int, [ct.c_void_p, ct.c_int32 * 2]),
     ("gila_opr_launches_per_apply", ct.c_int, [ct.c_void_p, ct.c_int64, ct.POINTER(ct.c_int64)]),
     ("gila_opr_cast", ct.c_int, [ct.c_void_p, ct.c_int, ct.POINTER(ct.c_void_p)]),
     ("gila_ls_solve", ct.c_int, [ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_void_p, ct.c_int64,

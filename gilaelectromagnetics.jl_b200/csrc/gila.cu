@@ -563,6 +563,30 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
     }
     best.y_tx = pick;
   }
+  // radix order of the x and y passes: the greedy one (radix-8 stages first)
+  // or its reverse, where they differ (specialised lengths, radix list not a
+  // palindrome); phases 0 and 2 hold both passes
+  for (int ax = 0; ax < 2 && e == cudaSuccess; ++ax) {
+    const AxisPlan& pl = c.plan[ax];
+    bool pal = true;
+    for (int k = 0; k < pl.nst; ++k) pal = pal && pl.radix[k] == pl.radix[pl.nst - 1 - k];
+    if (ct_tiles(cs, pl.P, false).empty() || pal) continue;
+    float bt = 1e30f;
+    int pick = 0;
+    for (int rv = 0; rv < 2; ++rv) {
+      Launch L = best;
+      (ax == 0 ? L.x_rev : L.y_rev) = rv;
+      const float t = time_of(L, {0, 2});
+      if (e != cudaSuccess) break;
+      if (tune_debug())
+        fprintf(stderr, "gila autotune dtype %d %c radix order %d: %.4f ms\n", (int)c.dtype, ax ? 'y' : 'x', rv, t);
+      if (t < bt) {
+        bt = t;
+        pick = rv;
+      }
+    }
+    (ax == 0 ? best.x_rev : best.y_rev) = pick;
+  }
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
   cudaFree(din);
@@ -1045,6 +1069,29 @@ gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]) {
   const int cs = (int)csize(c.dtype);
   if (tiles[2] > 0) L.y_tx = ct_tile_pick(cs, c.geom.P[1], tiles[2], false) == tiles[2] ? tiles[2] : L.y_tx;
   if (tiles[3] > 0) L.z_tx = ct_tile_pick(cs, c.geom.P[2], tiles[3], true) == tiles[3] ? tiles[3] : L.z_tx;
+  c.launch = L;
+  c.tuned = true;
+  return GILA_OK;
+}
+
+gila_status gila_opr_get_schedule(gila_opr* opr, int32_t sched[2]) {
+  if (!opr || !sched) return fail(GILA_ERR_ARG, "null argument");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  const Launch L = c.tuned ? c.launch : default_launch(c);
+  sched[0] = L.x_rev;
+  sched[1] = L.y_rev;
+  return GILA_OK;
+}
+
+gila_status gila_opr_set_schedule(gila_opr* opr, const int32_t sched[2]) {
+  if (!opr || !sched) return fail(GILA_ERR_ARG, "null argument");
+  if (sched[0] > 1 || sched[1] > 1) return fail(GILA_ERR_ARG, "radix order is 0 (greedy) or 1 (reversed)");
+  Core& c = *opr->core;
+  std::lock_guard<std::mutex> lk(c.mu);
+  Launch L = c.tuned ? c.launch : default_launch(c);
+  if (sched[0] >= 0) L.x_rev = sched[0];
+  if (sched[1] >= 0) L.y_rev = sched[1];
   c.launch = L;
   c.tuned = true;
   return GILA_OK;

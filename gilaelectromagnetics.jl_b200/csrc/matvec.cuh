@@ -71,6 +71,8 @@ struct Launch {
   int xi_lines;  // lines per CTA, x inverse
   int y_tx;      // kx tile, y passes
   int z_tx;      // kx tile, z pass
+  int x_rev = 0;  // radix order of the x passes: 0 greedy (8s first), 1 reversed
+  int y_rev = 0;  // radix order of the y passes
 };
 
 // Lippmann-Schwinger epilogue of the last pass (self operators): out =

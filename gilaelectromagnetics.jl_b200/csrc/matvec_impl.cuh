@@ -409,7 +409,7 @@ __global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
 // The same five passes with the transform length P, tile width and thread
 // count as template constants (see fft_ct.cuh).
 
-template <typename C, int P>
+template <typename C, int P, bool REV>
 __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd_ct(const XfParams<C> p) {
   constexpr int M = ct_xlines<sizeof(C)>(P);
   constexpr int T = ct_threads(M, P);
@@ -441,14 +441,14 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd
     const int64_t g = g0 + l;
     if (g < rows) A[g * P + i] = v;
   };
-  ct_run<C, P, 8, T, M, false, false>(p.tw, ldf, lds, sts, stg, true, false);
+  ct_run_range<C, P, 0, 0, ct_nst(P), 8, T, M, false, false, REV>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
 // FP32 x passes on row pairs: rows 2p and 2p+1 interleaved in shared memory
 // (float4 slot = element i of both rows, slot i + i/8 of the pair's row), so
 // every stage access is a conflict-free 16-byte transaction -- the access
 // pattern of the FP64 passes -- and the two rows share twiddles.
-template <int P>
+template <int P, bool REV>
 __global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xfwd2_ct(const XfParams<float2> p) {
   constexpr int M = ct_xlines2<8>(P);  // rows per CTA (even)
   constexpr int M2 = M / 2;
@@ -485,10 +485,10 @@ __global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xfwd2_ct(c
     if (g < rows) A[g * P + i] = make_float2(v.x, v.y);
     if (g + 1 < rows) A[(g + 1) * P + i] = make_float2(v.z, v.w);
   };
-  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, false, false, false>(p.tw, ldf, lds, sts, stg, true, false);
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, false, REV, false>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
-template <int P>
+template <int P, bool REV>
 __global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xinv2_ct(const XiParams<float2> p) {
   constexpr int M = ct_xlines2<8>(P);
   constexpr int M2 = M / 2;
@@ -532,10 +532,10 @@ __global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xinv2_ct(c
       out[o] = ls ? ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, w) : w;
     }
   };
-  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, true, false, false>(p.tw, lds, lds, sts, stg, true, false);
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, true, REV, false>(p.tw, lds, lds, sts, stg, true, false);
 }
 
-template <typename C, int P, bool INV, int TX>
+template <typename C, int P, bool INV, int TX, bool REV>
 __global__ void __launch_bounds__(ct_threads(TX, P)) k_y_ct(const YParams<C> p) {
   constexpr int T = ct_threads(TX, P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -564,11 +564,11 @@ __global__ void __launch_bounds__(ct_threads(TX, P)) k_y_ct(const YParams<C> p) 
   auto stg = [=](int t, int i, C v) {
     if (t < tmax && i < nout) dst[(int64_t)i * Px + t] = v;
   };
-  ct_run<C, P, 8, T, TX, INV, true>(p.tw, ldf, lds, sts, stg, true, false);
+  ct_run_range<C, P, 0, 0, ct_nst(P), 8, T, TX, INV, true, REV>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
 // FP32 y pass on line pairs (ct_stage2): two adjacent kx columns per task.
-template <int P, bool INV, int TX>
+template <int P, bool INV, int TX, bool REV>
 __global__ void __launch_bounds__(ct_threads2(TX, P)) k_y2_ct(const YParams<float2> p) {
   constexpr int T = ct_threads2(TX, P);
   constexpr int M2 = TX / 2;
@@ -599,7 +599,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P)) k_y2_ct(const YParams<floa
   auto stg = [=](int t2, int i, float4 v) {
     if (2 * t2 < tmax && i < nout) reinterpret_cast<float4*>(dst + (int64_t)i * Px)[t2] = v;
   };
-  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, INV, false, true>(p.tw, ldf, lds, sts, stg, true, false);
+  ct_run_range2<P, 0, 0, ct_nst(P), T, M2, INV, REV, true>(p.tw, ldf, lds, sts, stg, true, false);
 }
 
 template <typename C, int P, int TX>
@@ -1161,7 +1161,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf_min_bloc
   }
 }
 
-template <typename C, int P, bool AXPBY>
+template <typename C, int P, bool AXPBY, bool REV>
 __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv_ct(const XiParams<C> p) {
   constexpr int M = ct_xlines<sizeof(C)>(P);
   constexpr int T = ct_threads(M, P);
@@ -1222,7 +1222,7 @@ __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv
     else
       out[o] = v;
   };
-  ct_run<C, P, 8, T, M, true, false>(p.tw, lds, lds, sts, stg, true, false);
+  ct_run_range<C, P, 0, 0, ct_nst(P), 8, T, M, true, false, REV>(p.tw, lds, lds, sts, stg, true, false);
 }
 
 // Lengths with specialised kernels.
@@ -1295,6 +1295,29 @@ static bool is_mixed(const AxisPlan& pl) {
     KERNEL<<<(unsigned)blocks, T, sm, st>>>(__VA_ARGS__);                                    \
   } while (0)
 
+// one launch of a compile-time x / y kernel in the chosen radix order
+template <int P, bool REV>
+static cudaError_t run_xfwd2(const XfParams<float2>& p, int T, size_t sm, int64_t blocks, cudaStream_t st) {
+  cudaError_t e = set_smem((const void*)k_xfwd2_ct<P, REV>, sm);
+  if (e != cudaSuccess) return e;
+  k_xfwd2_ct<P, REV><<<(unsigned)blocks, T, sm, st>>>(p);
+  return cudaGetLastError();
+}
+template <int P, bool REV>
+static cudaError_t run_xinv2(const XiParams<float2>& p, int T, size_t sm, int64_t blocks, cudaStream_t st) {
+  cudaError_t e = set_smem((const void*)k_xinv2_ct<P, REV>, sm);
+  if (e != cudaSuccess) return e;
+  k_xinv2_ct<P, REV><<<(unsigned)blocks, T, sm, st>>>(p);
+  return cudaGetLastError();
+}
+template <int P, bool INV, int TX, bool REV>
+static cudaError_t run_y2(const YParams<float2>& p, int T, size_t sm, int64_t blocks, cudaStream_t st) {
+  cudaError_t e = set_smem((const void*)k_y2_ct<P, INV, TX, REV>, sm);
+  if (e != cudaSuccess) return e;
+  k_y2_ct<P, INV, TX, REV><<<(unsigned)blocks, T, sm, st>>>(p);
+  return cudaGetLastError();
+}
+
 template <typename C>
 cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* A, int64_t rows,
                         cudaStream_t st) {
@@ -1317,10 +1340,8 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
       const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                         \
       p.M = M;                                                                         \
       const int64_t blocks = (p.rows + M - 1) / M;                                     \
-      cudaError_t e2 = set_smem((const void*)k_xfwd2_ct<n>, sm);                       \
-      if (e2 != cudaSuccess) return e2;                                                \
-      k_xfwd2_ct<n><<<(unsigned)blocks, T2, sm, st>>>(xfp32(p));                       \
-      return cudaGetLastError();                                                       \
+      return L.x_rev ? run_xfwd2<n, true>(xfp32(p), T2, sm, blocks, st)               \
+                     : run_xfwd2<n, false>(xfp32(p), T2, sm, blocks, st);             \
     }                                                                                  \
   }                                                                                    \
   if (p.P == n) {                                                                      \
@@ -1329,7 +1350,10 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
     const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                           \
     p.M = M;                                                                           \
     const int64_t blocks = (p.rows + M - 1) / M;                                       \
-    GILA_LAUNCH(false, (k_xfwd_ct<C, n>), p);                                          \
+    if (L.x_rev)                                                                       \
+      GILA_LAUNCH(false, (k_xfwd_ct<C, n, true>), p);                                  \
+    else                                                                               \
+      GILA_LAUNCH(false, (k_xfwd_ct<C, n, false>), p);                                 \
     return cudaGetLastError();                                                         \
   }
     GILA_CT_SIZES(GILA_CT_XF)
@@ -1347,7 +1371,8 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
 }
 
 template <typename C, bool INV>
-static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, cudaStream_t st) {
+static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, bool rev,
+                                cudaStream_t st) {
   if (ct_has(p.P)) {
 #define GILA_CT_Y2(n, tx)                                  \
   if constexpr (ct_y_ok(sizeof(C), n, tx)) {               \
@@ -1355,14 +1380,14 @@ static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, 
       if constexpr (sizeof(C) == 8) {                      \
         if (zpair()) {                                     \
           const int T2 = ct_threads2(tx, n);               \
-          const void* fn2 = (const void*)k_y2_ct<n, INV, tx>; \
-          cudaError_t e2 = set_smem(fn2, sm);              \
-          if (e2 != cudaSuccess) return e2;                \
-          k_y2_ct<n, INV, tx><<<(unsigned)blocks, T2, sm, st>>>(yp32(p)); \
-          return cudaSuccess;                              \
+          return rev ? run_y2<n, INV, tx, true>(yp32(p), T2, sm, blocks, st) \
+                     : run_y2<n, INV, tx, false>(yp32(p), T2, sm, blocks, st); \
         }                                                  \
       }                                                    \
-      GILA_LAUNCH(false, (k_y_ct<C, n, INV, tx>), p);      \
+      if (rev)                                             \
+        GILA_LAUNCH(false, (k_y_ct<C, n, INV, tx, true>), p); \
+      else                                                 \
+        GILA_LAUNCH(false, (k_y_ct<C, n, INV, tx, false>), p); \
       return cudaSuccess;                                  \
     }                                                      \
   }
@@ -1421,7 +1446,8 @@ cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv
   const size_t sm = (size_t)p.TX * p.P * sizeof(C);
   const bool mx = is_mixed(d.plan[1]);
   const int64_t blocks = (int64_t)p.ntiles * nq;
-  cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, st) : launch_y_one<C, false>(p, mx, T, sm, blocks, st);
+  cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, L.y_rev != 0, st)
+                      : launch_y_one<C, false>(p, mx, T, sm, blocks, L.y_rev != 0, st);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
@@ -1511,7 +1537,8 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
 }
 
 template <typename C, bool AXPBY>
-static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, cudaStream_t st) {
+static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, bool rev,
+                                   cudaStream_t st) {
   if (ct_has(p.P)) {
 #define GILA_CT_XI(n)                                                    \
   if constexpr (sizeof(C) == 8 && !AXPBY) {                              \
@@ -1520,14 +1547,15 @@ static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t 
       const int T2 = ct_threads2(M2r, n);                                \
       const size_t sm2 = (size_t)M2r * row_stride(n) * sizeof(C);        \
       const int64_t blocks2 = (p.rows + M2r - 1) / M2r;                  \
-      cudaError_t e2 = set_smem((const void*)k_xinv2_ct<n>, sm2);        \
-      if (e2 != cudaSuccess) return e2;                                  \
-      k_xinv2_ct<n><<<(unsigned)blocks2, T2, sm2, st>>>(xip32(p));       \
-      return cudaSuccess;                                                \
+      return rev ? run_xinv2<n, true>(xip32(p), T2, sm2, blocks2, st)    \
+                 : run_xinv2<n, false>(xip32(p), T2, sm2, blocks2, st);  \
     }                                                                    \
   }                                                                      \
   if (p.P == n) {                                                        \
-    GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY>), p);                     \
+    if (rev)                                                             \
+      GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY, true>), p);             \
+    else                                                                 \
+      GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY, false>), p);            \
     return cudaSuccess;                                                  \
   }
     GILA_CT_SIZES(GILA_CT_XI)
@@ -1588,7 +1616,8 @@ cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const
   const bool mx = is_mixed(d.plan[0]);
   const int64_t blocks = (p.rows + p.M - 1) / p.M;
   cudaError_t e =
-      axpby ? launch_xinv_one<C, true>(p, mx, T, sm, blocks, st) : launch_xinv_one<C, false>(p, mx, T, sm, blocks, st);
+      axpby ? launch_xinv_one<C, true>(p, mx, T, sm, blocks, L.x_rev != 0, st)
+            : launch_xinv_one<C, false>(p, mx, T, sm, blocks, L.x_rev != 0, st);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }

@@ -16,7 +16,8 @@
  *    GILA_C64 (ComplexF32).  Multi-RHS batches are contiguous, one vector after
  *    the other.
  *  - Pointers may be host or device memory; the library tells them apart with
- *    cudaPointerGetAttributes.  Host buffers are staged through pinned memory.
+ *    cudaPointerGetAttributes.  Host buffers are copied through device
+ *    staging buffers (page-locked host buffers let the copies overlap).
  *  - No call aborts; every call returns a gila_status.  gila_last_error()
  *    returns a message for the last failure on the calling thread.
  *  - Calls that take a `stream` (a cudaStream_t; NULL = the operator's own
@@ -165,7 +166,8 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 
 /* Launch shapes.  tiles = {x-forward lines per CTA, x-inverse lines per CTA,
  * y-pass kx tile, z-pass kx tile}.  No counterpart in the reference.  The
- * first apply of an operator picks the y and z tiles by timing every compiled
+ * first apply of an operator picks the y and z tiles (and the radix order of
+ * the x and y transforms, gila_opr_get_schedule) by timing every compiled
  * candidate on the operator's workspaces (cached per context and geometry;
  * GILA_AUTOTUNE=0 keeps the defaults); gila_opr_autotune re-runs that for a
  * batch of nrhs vectors; gila_opr_set_tiles forces tiles (entries <= 0 or
@@ -174,6 +176,15 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 gila_status gila_opr_autotune(gila_opr* opr, int64_t nrhs, int32_t tiles[4]);
 gila_status gila_opr_get_tiles(gila_opr* opr, int32_t tiles[4]);
 gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]);
+
+/* Radix order of the x and y transforms at the specialised lengths (no
+ * counterpart in the reference, whose FFTs are FFTW / CUFFT plans): sched =
+ * {x, y}, 0 = the greedy order (radix-8 stages first), 1 = its reverse.  Both
+ * compute the same transform; results differ by rounding only.  The autotuner
+ * picks them together with the tiles; set forces them (entries < 0 keep the
+ * current value). */
+gila_status gila_opr_get_schedule(gila_opr* opr, int32_t sched[2]);
+gila_status gila_opr_set_schedule(gila_opr* opr, const int32_t sched[2]);
 
 /* Number of kernels one apply of nrhs vectors launches. */
 gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n);

@@ -85,3 +85,22 @@ def test_ct_multi_rhs(dtype, case):
     mem.apply_into(X, Y, nrhs=3)
     for k in range(3):
         assert np.array_equal(Y[..., k], gila.egoOpr(mem, xs[k]))
+
+
+@pytest.mark.parametrize("case", [CT_CASES[1], CT_CASES[2], CT_CASES[6]], ids=lambda c: f"{c[0]}<-{c[1]}")
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_ct_radix_orders(case, dtype):
+    """Both radix orders of the x and y transforms (greedy, reversed): the
+    same transform, so every combination matches the oracle."""
+    gila = load_pkg()
+    mix, mem, ref = _build(gila, case, dtype)
+    x = np.asfortranarray(seeded_current(mix.src_cel, 23).astype(dtype))
+    y_ref = ego_opr(ref, x.astype(np.complex128))
+    tol = TOL_F64 if dtype == np.complex128 else TOL_F32
+    for xr in (0, 1):
+        for yr in (0, 1):
+            mem.schedule = (xr, yr)
+            assert mem.schedule == (xr, yr)
+            assert rel_l2(gila.egoOpr(mem, x), y_ref) <= tol
+    with pytest.raises(gila.GilaError):
+        mem.schedule = (2, 0)
