@@ -194,6 +194,18 @@ def make_opr(gila, cel, dtype, seed=1, src_cel=None, trg_org=(0, 0, 0), src_org=
     return mem, tru
 
 
+def job_rate(dist, ms_local, steps, world, device="cuda"):
+    """Whole-job rate of `world` replicas that each ran `steps` units in
+    ms_local device milliseconds: units / the max over ranks of the time (an
+    all-reduce every rank takes).  Returns (units per second, max ms)."""
+    import torch
+    t = torch.tensor([float(ms_local)], dtype=torch.float64, device=device)
+    if dist is not None:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    return world * steps / (ms_max / 1e3), ms_max
+
+
 def device_rate(torch, mem, cel_in, cel_out, tdt, steps, warmup, stream, flush, seed=3, clk=None):
     """matvec/s with device-resident vectors; per-step CUDA events, L2
     flushed between steps (outside the events)."""
@@ -275,11 +287,7 @@ def main():
     clk = Clocks(local)
     ms, y_dev = device_rate(torch, mem, CEL, CEL, tdt, a.steps, W, stream, flush, clk=clk)
     clocks = clk.stop()
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = world * a.steps / (ms_max / 1e3)
+    value, ms_max = job_rate(dist, ms, a.steps, world)
 
     # ---- e2e: public API with pinned host buffers, copies inside the timed
     # region.  The host vectors go to the API E2E_BATCH at a time; the call
@@ -305,11 +313,7 @@ def main():
         done += n
     e1.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = e0.elapsed_time(e1)
-    t = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    e2e_value = world * a.steps / (float(t.item()) / 1e3)
+    e2e_value, _ = job_rate(dist, e0.elapsed_time(e1), a.steps, world)
     nbytes = xh[0].numel() * xh.element_size()
 
     # ---- roofline of the dominant kernel (z pass), timed live
