@@ -244,10 +244,11 @@ def main():
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline (profiling runs)")
     ap.add_argument("--dtype", default="c128", choices=["c128", "c64"],
                     help="precision of the main matvec workload (c64: ComplexF32, for profiling)")
-    ap.add_argument("--profile", choices=["solve", "build"], default=None,
-                    help="run a small bounded workload for a profiler's launch list instead of the bench: "
-                         "'solve' = two short mixed-precision solves on 96x96x48, 'build' = the GPU kernel "
-                         "build of a 32^3 self operator; prints no bench line")
+    ap.add_argument("--profile", choices=["solve", "build", "matvec256"], default=None,
+                    help="run a small bounded workload for a profiler instead of the bench: 'solve' = two "
+                         "short mixed-precision solves on 96x96x48, 'build' = the GPU kernel build of a 32^3 "
+                         "self operator, 'matvec256' = 4 matvecs of the 256x256x128 self operator in the "
+                         "precision of --dtype; prints no bench line")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the Poisson stream and of the burst that measures saturation")
     a = ap.parse_args()
@@ -260,7 +261,7 @@ def main():
             return 0
         return run_reference(a, world)
     if a.profile:
-        return run_profile(a.profile)
+        return run_profile(a.profile, a.dtype)
 
     import torch
     torch.cuda.set_device(local)
@@ -638,7 +639,7 @@ def oracle_check(gila, x, y_ref):
     return out
 
 
-def run_profile(kind):
+def run_profile(kind, dtype="c128"):
     """Small bounded workloads whose every kernel a profiler's launch list
     can cover: the Krylov-cycle kernels of the solver (two solves of 12
     matvecs, ComplexF32 with FP64 reliable updates, on 96x96x48 with a slab
@@ -646,6 +647,17 @@ def run_profile(kind):
     kernel build (32^3 self operator, intOrd 16)."""
     import torch
     gila = load_pkg()
+    if kind == "matvec256":
+        cel = (256, 256, 128)
+        ndt, tdt = (np.complex64, torch.complex64) if dtype == "c64" else (np.complex128, torch.complex128)
+        mem, _ = make_opr(gila, cel, ndt)
+        g = torch.Generator(device="cuda").manual_seed(3)
+        x = torch.randn((3, cel[2], cel[1], cel[0]), dtype=tdt, device="cuda", generator=g)
+        y = torch.empty_like(x)
+        for _ in range(4):
+            mem.apply_into(x, y)
+        torch.cuda.synchronize()
+        return 0
     if kind == "build":
         opt = gila.GlaKerOpt(1.0 + 0j, 16, False, True, (), ())
         gila.GlaOprMem(opt, gila.GlaVol((32, 32, 32), SCL))
