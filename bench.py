@@ -249,6 +249,8 @@ def main():
                          "short mixed-precision solves on 96x96x48, 'build' = the GPU kernel build of a 32^3 "
                          "self operator, 'matvec256' = 4 matvecs of the 256x256x128 self operator in the "
                          "precision of --dtype; prints no bench line")
+    ap.add_argument("--serve-burst", type=int, default=200,
+                    help="requests of the burst that measures saturation (at most --serve-requests)")
     ap.add_argument("--serve-requests", type=int, default=40,
                     help="requests of the Poisson stream and of the burst that measures saturation")
     a = ap.parse_args()
@@ -357,7 +359,7 @@ def main():
     if not a.no_solve and world == 1:
         out["solve"] = solve_bench(torch, gila)
     if not a.no_serve and world == 1:
-        out["serve"] = serve_bench(gila, a.serve_requests)
+        out["serve"] = serve_bench(gila, a.serve_requests, a.serve_burst)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -534,12 +536,12 @@ def serve_request(cel, rng):
     return chi, b
 
 
-def serve_bench(gila, n_stream):
+def serve_bench(gila, n_stream, n_burst=200):
     """The request stream: solves of volumes drawn uniformly from
     SERVE_SHAPES (1/32-wavelength cells), each with its own medium and
     incident wave, tol 1e-6, ComplexF32 Krylov with FP64 reliable updates.
-    A burst of min(n_stream, 200) requests (submitted at once) measures the
-    saturation throughput; then n_stream requests drawn the same way arrive
+    A burst of min(n_stream, n_burst) requests (submitted at once) measures
+    the saturation throughput; then n_stream requests drawn the same way arrive
     as a Poisson process at 80% of it (seeded).
     Inputs come from a pool of 3 seeded variants per shape."""
     rng = np.random.default_rng(11)
@@ -557,7 +559,7 @@ def serve_bench(gila, n_stream):
             alone["x".join(map(str, c))].update({"ms": round(lat, 1), "cycles": inf.iters})
         res["alone"] = alone
         # saturation: a burst
-        nb = max(4, min(n_stream, 200))
+        nb = max(4, min(n_stream, n_burst))
         picks = [SERVE_SHAPES[i] for i in rng.integers(0, len(SERVE_SHAPES), nb)]
         t0 = time.perf_counter()
         tk = [srv.submit(c, SCL, *pool[c][int(rng.integers(0, 3))]) for c in picks]

@@ -18,6 +18,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
+#include <cstdlib>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -85,6 +87,32 @@ size_t self_op_bytes(const gila_vol& v, bool mixed) {
     k *= (size_t)std::max<int64_t>((n + 1) / 2 + (n % 2 == 0 ? 1 : 0), 2);
   }
   return k * (16 + (mixed ? 8 : 0));
+}
+
+// Stream priority of a shape's batch: volumes of at most 2^17 cells get the
+// device's highest priority, up to 2^19 cells the next one, larger volumes
+// the default, which they share.  A small request's Krylov cycle (tens of
+// microseconds of kernels) then waits for free SMs, not behind a large
+// batch's queued kernels; large shapes are not ranked among themselves (a
+// large shape below another one would starve: its cycles are long and the
+// other's never stop).  GILA_SERVER_PRIORITY=0 gives every batch the default
+// priority.
+int shape_priority(const gila_vol& v) {
+  static const bool on = [] {
+    const char* e = getenv("GILA_SERVER_PRIORITY");
+    return !(e && e[0] == '0');
+  }();
+  if (!on) return 0;
+  int least = 0, greatest = 0;
+  if (cudaDeviceGetStreamPriorityRange(&least, &greatest) != cudaSuccess) {
+    cudaGetLastError();
+    return 0;
+  }
+  double cells = 1.0;
+  for (int d = 0; d < 3; ++d) cells *= (double)v.cel[d];
+  if (cells > (double)(1 << 19)) return least;
+  const int p = greatest + (cells > (double)(1 << 17) ? 1 : 0);
+  return p > least ? least : p;
 }
 
 size_t build_tmp_bytes(const gila_vol& v) {
@@ -279,7 +307,9 @@ struct Server {
           continue;
         }
         std::unique_ptr<LsBatch> b;
-        const gila_status s = make_ls_batch(*sh->g64, sh->g32.get(), S, cfg, b);
+        BatchCfg bc = cfg;
+        bc.priority = shape_priority(sh->vol);
+        const gila_status s = make_ls_batch(*sh->g64, sh->g32.get(), S, bc, b);
         if (s != GILA_OK) {
           gila_solve_info inf{};
           complete(rq, s, gila_last_error(), inf);

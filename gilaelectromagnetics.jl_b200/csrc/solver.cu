@@ -663,7 +663,7 @@ class LsBatchT final : public LsBatch {
   }
 
   gila_status init() {
-    GILA_CUDA_TRY(cudaStreamCreateWithFlags(&s_, cudaStreamNonBlocking));
+    GILA_CUDA_TRY(cudaStreamCreateWithPriority(&s_, cudaStreamNonBlocking, cfg_.priority));
     GILA_CUDA_TRY(cudaEventCreateWithFlags(&ev_, cudaEventDisableTiming));
     const size_t vb = (size_t)S_ * n_;
     const bool mixed = cfg_.mixed != 0;

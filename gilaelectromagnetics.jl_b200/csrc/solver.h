@@ -25,6 +25,7 @@ struct BatchCfg {
   int mixed = 0;       // Krylov process on the ComplexF32 operator
   int graph = 1;       // replay cycles from captured CUDA graphs
   int chi_shared = 0;  // one medium for all slots (set_shared_chi)
+  int priority = 0;    // CUDA stream priority of the batch's stream (lower = more urgent)
 };
 
 struct SlotResult {
