@@ -389,6 +389,30 @@ def sweep(torch, gila, stream, flush, y64):
             "ms": round(ms / 10, 4), "matvec_per_s": round(1e4 / ms, 2),
             "tmin_frac": round(tmin_bytes(src, trg, tru, cs) / (ms / 10 / 1e3) / 1e9 / peak, 4)}
         del mem
+    # four vectors per apply (batched launches), per-vector time, L2 flushed between applies
+    for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
+        mem, tru = make_opr(gila, CEL, dt)
+        nb = 4
+        g = torch.Generator(device="cuda").manual_seed(5)
+        xb = torch.randn((nb, 3, CEL[2], CEL[1], CEL[0]), dtype=tdt, device="cuda", generator=g)
+        yb = torch.empty_like(xb)
+        mem.autotune(nb)
+        for _ in range(3):
+            mem.apply_into(xb, yb, nrhs=nb, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(10)]
+        with torch.cuda.stream(stream):
+            for e0, e1 in evs:
+                flush.zero_()
+                e0.record(stream)
+                mem.apply_into(xb, yb, nrhs=nb, stream=stream.cuda_stream)
+                e1.record(stream)
+        torch.cuda.synchronize()
+        ms = sum(a.elapsed_time(b) for a, b in evs) / (10 * nb)
+        res[f"self_128x128x64_{np.dtype(dt).name}_4_per_apply"] = {
+            "ms_per_vector": round(ms, 4), "matvec_per_s": round(1e3 / ms, 2),
+            "tmin_frac": round(tmin_bytes(CEL, CEL, tru, cs) / (ms / 1e3) / 1e9 / peak, 4)}
+        del mem, xb, yb
     # 256x256x128 (north-star roofline target)
     big = (256, 256, 128)
     for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
