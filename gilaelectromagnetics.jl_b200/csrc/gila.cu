@@ -490,20 +490,19 @@ static bool tune_debug() {
   return e && e[0] == '1';
 }
 
+// Times the candidates for nrhs vectors on the given buffers: din (finite,
+// nrhs input vectors, read only), dout (nrhs output vectors, overwritten),
+// workspaces A and B laid out for g, all on stream s.
 template <typename C>
-static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
-  const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
-  C *din = nullptr, *dout = nullptr;
-  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
-  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
-  if (e != cudaSuccess) {
-    cudaFree(din);
-    return cuda_fail(e, "cudaMalloc");
-  }
-  cudaMemsetAsync(din, 0, (size_t)ni * sizeof(C), c.stream);
+static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C* dout, C* A, C* B,
+                           cudaStream_t s, Launch& best) {
+  cudaError_t e = cudaSuccess;
   cudaEvent_t ev[2];
-  cudaEventCreate(&ev[0]);
-  cudaEventCreate(&ev[1]);
+  GILA_CUDA_TRY(cudaEventCreate(&ev[0]));
+  if ((e = cudaEventCreate(&ev[1])) != cudaSuccess) {
+    cudaEventDestroy(ev[0]);
+    return cuda_fail(e, "cudaEventCreate");
+  }
   const DevOp<C> d = devop<C>(c);
   C one, zero;
   one.x = 1;
@@ -514,13 +513,12 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
   auto time_of = [&](const Launch& L, std::initializer_list<int> phases) -> float {
     float bt = 1e30f;
     for (int r = 0; r < 4 && e == cudaSuccess; ++r) {
-      cudaEventRecord(ev[0], c.stream);
+      cudaEventRecord(ev[0], s);
       for (int ph : phases) {
-        e = launch_matvec_phase<C>(ph, c.geom, d, L, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B),
-                                   (int)nrhs, false, one, zero, c.stream);
+        e = launch_matvec_phase<C>(ph, g, d, L, din, dout, A, B, (int)nrhs, false, one, zero, s);
         if (e != cudaSuccess) break;
       }
-      cudaEventRecord(ev[1], c.stream);
+      cudaEventRecord(ev[1], s);
       cudaEventSynchronize(ev[1]);
       float t = 0;
       cudaEventElapsedTime(&t, ev[0], ev[1]);
@@ -589,11 +587,61 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
   }
   cudaEventDestroy(ev[0]);
   cudaEventDestroy(ev[1]);
-  cudaFree(din);
-  cudaFree(dout);
   if (e != cudaSuccess) return cuda_fail(e, "autotune");
   return GILA_OK;
 }
+
+// the operator's own workspaces and two scratch vectors
+template <typename C>
+static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
+  const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
+  C *din = nullptr, *dout = nullptr;
+  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
+  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
+  if (e == cudaSuccess) e = cudaMemsetAsync(din, 0, (size_t)ni * sizeof(C), c.stream);
+  if (e != cudaSuccess) {
+    cudaFree(din);
+    cudaFree(dout);
+    return cuda_fail(e, "autotune buffers");
+  }
+  const gila_status s =
+      tune_on<C>(c, c.geom, nrhs, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B), c.stream, best);
+  cudaStreamSynchronize(c.stream);
+  cudaFree(din);
+  cudaFree(dout);
+  return s;
+}
+
+static bool autotune_off() {
+  const char* ev = getenv("GILA_AUTOTUNE");
+  return ev && ev[0] == '0';
+}
+
+template <typename C>
+gila_status tuned_launch(Core& c, const Geom& g, int64_t nrhs, const C* din, C* dout, C* A, C* B, cudaStream_t s,
+                         Launch& L) {
+  {
+    std::lock_guard<std::mutex> lk(c.ctx->mu);
+    auto it = c.ctx->tune_cache.find(tune_key(c, nrhs));
+    if (it != c.ctx->tune_cache.end()) {
+      L = it->second;
+      return GILA_OK;
+    }
+  }
+  if (autotune_off()) {
+    L = default_launch(c);
+    return GILA_OK;
+  }
+  const gila_status st = tune_on<C>(c, g, nrhs, din, dout, A, B, s, L);
+  if (st != GILA_OK) return st;
+  std::lock_guard<std::mutex> lk(c.ctx->mu);
+  c.ctx->tune_cache[tune_key(c, nrhs)] = L;
+  return GILA_OK;
+}
+template gila_status tuned_launch<double2>(Core&, const Geom&, int64_t, const double2*, double2*, double2*,
+                                           double2*, cudaStream_t, Launch&);
+template gila_status tuned_launch<float2>(Core&, const Geom&, int64_t, const float2*, float2*, float2*, float2*,
+                                          cudaStream_t, Launch&);
 
 gila_status autotune(Core& c, int64_t nrhs) {
   gila_status s = ensure_work(c, nrhs);
@@ -624,8 +672,7 @@ gila_status ensure_tuned(Core& c, int64_t nrhs) {
       return GILA_OK;
     }
   }
-  const char* ev = getenv("GILA_AUTOTUNE");
-  if (ev && ev[0] == '0') {
+  if (autotune_off()) {
     c.launch = default_launch(c);
     c.tuned = true;
     return GILA_OK;

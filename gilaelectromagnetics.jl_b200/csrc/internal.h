@@ -108,6 +108,12 @@ void release_work(Core& c);  // frees the matvec workspaces (allocated again on 
 // launch shapes: cached per context, else timed (autotune) at first use
 gila_status ensure_tuned(Core& c, int64_t nrhs);
 gila_status autotune(Core& c, int64_t nrhs);
+// launch shapes for nrhs vectors laid out for g: the context's cached choice,
+// else timed on the caller's buffers (din finite and read only, dout
+// overwritten, workspaces A and B) on stream s and cached; c.launch unchanged
+template <typename C>
+gila_status tuned_launch(Core& c, const Geom& g, int64_t nrhs, const C* din, C* dout, C* A, C* B, cudaStream_t s,
+                         Launch& L);
 int64_t in_elems(const Core& c);
 int64_t out_elems(const Core& c);
 bool is_device_ptr(const void* p);

@@ -605,6 +605,7 @@ struct OpRef {  // an operator with workspaces owned by a batch
   C* A;
   C* B;
   int cap;      // right-hand sides per matvec launch sequence
+  Launch launch;  // launch shapes for cap right-hand sides
 };
 
 // right-hand sides the FP64 workspace of a mixed batch holds: reliable
@@ -722,6 +723,24 @@ class LsBatchT final : public LsBatch {
     }
     // every Krylov vector starts finite
     GILA_CUDA_TRY(cudaMemsetAsync(base, 0, (size_t)nvec * vb * sizeof(CI), s_));
+    // launch shapes for the batch's own right-hand-side counts: the tile
+    // widths and radix orders that win for one vector need not win for a
+    // chunk of several.  Timed on zero vectors (G 0 = 0 leaves every
+    // buffer finite), or the operators' own single-vector choice.
+    op64_.launch = g64_.launch;
+    opi_.launch = gi_.launch;
+    if (cfg_.tune) {
+      gila_status st;
+      GILA_CUDA_TRY(cudaMemsetAsync(x64_, 0, vb * sizeof(double2), s_));
+      if ((st = tuned_launch<double2>(g64_, op64_.geom, op64_.cap, x64_, r64_, op64_.A, op64_.B, s_,
+                                      op64_.launch)) != GILA_OK)
+        return st;
+      if (!mixed)
+        opi_.launch = op64_.launch;
+      else if ((st = tuned_launch<CI>(gi_, opi_.geom, opi_.cap, base, kv_.r[0], opi_.A, opi_.B, s_,
+                                      opi_.launch)) != GILA_OK)
+        return st;
+    }
     GILA_CUDA_TRY(cudaMemcpyAsync(st_d_, st_h_, (size_t)S_ * sizeof(Stat), cudaMemcpyHostToDevice, s_));
     k_shadow<CI><<<nb_, kT, 0, s_>>>(shadow_, n_, 0x5EEDull);
     GILA_CUDA_TRY(cudaGetLastError());
@@ -912,7 +931,7 @@ class LsBatchT final : public LsBatch {
     zero.y = 0;
     for (auto [r0, r1] : runs_of(m, op.cap)) {
       LsEpi<C> ep{in + (size_t)r0 * n_, chi ? chi + (size_t)r0 * chi_rs() : nullptr, chi_rs()};
-      GILA_CUDA_TRY(launch_matvec<C>(op.geom, devop<C>(*op.core), op.core->launch, in + (size_t)r0 * n_,
+      GILA_CUDA_TRY(launch_matvec<C>(op.geom, devop<C>(*op.core), op.launch, in + (size_t)r0 * n_,
                                      out + (size_t)r0 * n_, op.A, op.B, r1 - r0, false, one, zero, s_,
                                      chi ? &ep : nullptr));
     }
@@ -1235,9 +1254,10 @@ gila_status make_ls_batch(Core& g64, Core* g32, int slots, const BatchCfg& cfg, 
   if (s != GILA_OK) return s;
   if (slots < 1 || slots > 65535) return fail(GILA_ERR_ARG, "slots must be in 1..65535");
   if (cfg.ell < 1 || cfg.ell > kMaxEll) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
-  // launch shapes of the operators (timed once per geometry, cached)
+  // launch shapes of the operators for one vector (timed once per geometry,
+  // cached): the batch's own choice when it does not time its chunks
   for (Core* c : {&g64, g32}) {
-    if (!c || c->tuned) continue;
+    if (!c || c->tuned || cfg.tune) continue;
     std::lock_guard<std::mutex> lk(c->mu);
     if ((s = ensure_tuned(*c, 1)) != GILA_OK) return s;
   }
@@ -1332,6 +1352,7 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   cfg.mixed = opts ? (opts->mixed != 0) : 0;
   cfg.graph = opts ? (opts->no_graph == 0) : 1;
   cfg.chi_shared = 1;
+  cfg.tune = 1;
   if (const char* ev = getenv("GILA_SOLVE_GRAPH"))
     if (ev[0] == '0') cfg.graph = 0;
   so.tol = opts && opts->tol > 0 ? opts->tol : 1e-6;

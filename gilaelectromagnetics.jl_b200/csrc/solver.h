@@ -26,6 +26,7 @@ struct BatchCfg {
   int graph = 1;       // replay cycles from captured CUDA graphs
   int chi_shared = 0;  // one medium for all slots (set_shared_chi)
   int priority = 0;    // CUDA stream priority of the batch's stream (lower = more urgent)
+  int tune = 0;        // time the launch shapes for the batch's own right-hand-side counts
 };
 
 struct SlotResult {
