@@ -473,8 +473,9 @@ def solve_bench(torch, gila):
     64 point-dipole right-hand sides on 96^3 with a centred 48^3 inclusion
     (chi ~ U[0,3] seeded) solved as one batch.  BiCGStab(2) to FP64 relative
     residual 1e-6; kernels built on the GPU; inputs device-resident; each
-    timed solve follows a short untimed one of the same shape that leaves the
-    batch's device state resident (keep=True), as a service would."""
+    timed solve follows a short untimed one of the same shape and variant
+    that leaves the batch's device state resident (keep=True), as a service
+    would."""
     res = {}
     opt = gila.GlaKerOpt(1.0 + 0j, 32, False, True, (), ())
     # thin film
@@ -490,9 +491,11 @@ def solve_bench(torch, gila):
     ls.g32()
     b = torch.from_numpy(np.ascontiguousarray(plane_wave(cel).reshape(-1, order="F"))).cuda()
     b = b.reshape(3, cel[2], cel[1], cel[0])
-    for mixed in (True, False):
-        _warm_solve(torch, gila, ls, b, mixed=mixed)
+    # the operator keeps one solve batch resident: each variant's timed solve
+    # directly follows its own warm-up
+    _warm_solve(torch, gila, ls, b, mixed=True)
     xm, im, msm = _timed_solve(torch, gila, ls, b, mixed=True, max_matvecs=20000, keep=True)
+    _warm_solve(torch, gila, ls, b, mixed=False)
     xp, ip, msp = _timed_solve(torch, gila, ls, b, mixed=False, max_matvecs=20000, keep=True)
     diff = float(torch.linalg.vector_norm(xm - xp) / torch.linalg.vector_norm(xp))
     res["film_256x256x128"] = {"kernel_build_s": round(tb, 2), "plain_fp64": _info(ip, msp),
@@ -524,12 +527,21 @@ def solve_bench(torch, gila):
     D = D.cuda()
     B = torch.empty_like(D)
     G.mem.apply_into(D, B, nrhs=nr)   # incident fields G d_j
+    # best of two timed solves per variant (each a few seconds), after the
+    # variant's own warm-up
+    runs = {True: [], False: []}
     for mixed in (True, False):
         _warm_solve(torch, gila, ls, B, mixed=mixed)
-    xm, im, msm = _timed_solve(torch, gila, ls, B, mixed=True, max_matvecs=20000, keep=True)
-    xp, ip, msp = _timed_solve(torch, gila, ls, B, mixed=False, max_matvecs=20000, keep=True)
+        for _ in range(2):
+            runs[mixed].append(_timed_solve(torch, gila, ls, B, mixed=mixed, max_matvecs=20000, keep=True))
+    xm, im, msm = min(runs[True], key=lambda r: r[2])
+    xp, ip, msp = min(runs[False], key=lambda r: r[2])
     res["dipoles_96cube_64rhs"] = {"plain_fp64": _info(ip, msp, nr), "mixed_c64_reliable": _info(im, msm, nr),
-                                   "speedup_mixed_vs_plain": round(msp / msm, 3)}
+                                   "speedup_mixed_vs_plain": round(msp / msm, 3),
+                                   "ms_each_run": {"plain_fp64": [round(r[2], 1) for r in runs[False]],
+                                                   "mixed_c64_reliable": [round(r[2], 1) for r in runs[True]]},
+                                   "timing": "best of two timed solves per variant"}
+    del runs
     del ls, G, xm, xp, B, D
     torch.cuda.empty_cache()
     return res
