@@ -318,6 +318,7 @@ def main():
     torch.cuda.synchronize()
     e2e_value, _ = job_rate(dist, e0.elapsed_time(e1), a.steps, world)
     nbytes = xh[0].numel() * xh.element_size()
+    copy_bound = pinned_copy_rate(torch, xh, yh)
 
     # ---- roofline of the dominant kernel (z pass), timed live
     passes = mem.time_passes(1, reps=max(3, min(a.steps, 10)))
@@ -345,7 +346,8 @@ def main():
                                + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
                    "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
         "e2e": {"value": round(e2e_value, 2), "unit": "matvec/s", "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors, 20 vectors per call (copies overlap the passes)"},
+                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors, 20 vectors per call (copies overlap the passes)",
+                "copy_bound": copy_bound, "frac_of_copy_bound": round(e2e_value / world / copy_bound["vectors_per_s"], 4)},
         "gpu_launches": int(mem.launches_per_apply(1)) * a.steps,
         "roofline": roofline,
         "clocks": clocks,
@@ -464,6 +466,37 @@ def _info(info, ms, nrhs=1):
     return {"ms": round(ms, 1), "solves_per_s": round(nrhs / (ms / 1e3), 3), "cycles": info.iters,
             "fp64_updates": info.outer, "matvecs_f64": info.matvecs_f64, "matvecs_f32": info.matvecs_f32,
             "rel_res_max": info.rel_res, "converged": info.converged}
+
+
+def pinned_copy_rate(torch, xh, yh, reps=3):
+    """The rate the host link allows the end-to-end path: the same pinned
+    vectors copied host -> device and device -> host at once (two streams,
+    no compute), best of reps, in vectors per second and GB/s per direction."""
+    k = xh.shape[0]
+    d_in = torch.empty_like(xh[0], device="cuda")
+    d_out = torch.empty_like(yh[0], device="cuda")
+    s_up, s_down = torch.cuda.Stream(), torch.cuda.Stream()
+    best = float("inf")
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record()
+        s_up.wait_event(e0)
+        s_down.wait_event(e0)
+        for i in range(k):
+            with torch.cuda.stream(s_up):
+                d_in.copy_(xh[i], non_blocking=True)
+            with torch.cuda.stream(s_down):
+                yh[i].copy_(d_out, non_blocking=True)
+        torch.cuda.current_stream().wait_stream(s_up)
+        torch.cuda.current_stream().wait_stream(s_down)
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    nb = xh[0].numel() * xh.element_size()
+    return {"vectors_per_s": round(k / best * 1e3, 1), "gbps_per_direction": round(nb * k / best / 1e6, 2),
+            "how": f"{k} pinned vectors uploaded and downloaded at once on two streams, no compute"}
 
 
 def solve_bench(torch, gila):

@@ -529,21 +529,29 @@ static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C
   const int cs = (int)csize(c.dtype);
   best = default_launch(c);
   std::vector<int> zc = ct_tiles(cs, c.geom.P[2], true), yc = ct_tiles(cs, c.geom.P[1], false);
-  if (zc.size() > 1) {
+  // z tile width jointly with the task form of the fused z pass (one task
+  // per thread slot, or one per mirror pair of z frequencies where the
+  // kernel has that form; the same arithmetic either way)
+  if (!zc.empty()) {
     float bt = 1e30f;
-    int pick = best.z_tx;
-    for (int tx : zc) {
-      Launch L = best;
-      L.z_tx = tx;
-      const float t = time_of(L, {1});
-      if (e != cudaSuccess) break;
-      if (tune_debug()) fprintf(stderr, "gila autotune dtype %d z tile %d: %.4f ms\n", (int)c.dtype, tx, t);
-      if (t < bt) {
-        bt = t;
-        pick = tx;
+    int pick = best.z_tx, pick_mir = best.z_mir;
+    for (int tx : zc)
+      for (int mir = 0; mir < 2 && e == cudaSuccess; ++mir) {
+        Launch L = best;
+        L.z_tx = tx;
+        L.z_mir = mir;
+        const float t = time_of(L, {1});
+        if (e != cudaSuccess) break;
+        if (tune_debug())
+          fprintf(stderr, "gila autotune dtype %d z tile %d mirror pairs %d: %.4f ms\n", (int)c.dtype, tx, mir, t);
+        if (t < bt) {
+          bt = t;
+          pick = tx;
+          pick_mir = mir;
+        }
       }
-    }
     best.z_tx = pick;
+    best.z_mir = pick_mir;
   }
   if (yc.size() > 1 && e == cudaSuccess) {
     float bt = 1e30f;

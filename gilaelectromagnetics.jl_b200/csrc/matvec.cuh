@@ -73,6 +73,7 @@ struct Launch {
   int z_tx;      // kx tile, z pass
   int x_rev = 0;  // radix order of the x passes: 0 greedy (8s first), 1 reversed
   int y_rev = 0;  // radix order of the y passes
+  int z_mir = 1;  // fused z pass: one task per mirror pair of z frequencies
 };
 
 // Lippmann-Schwinger epilogue of the last pass (self operators): out =

@@ -165,6 +165,7 @@ struct ZParams {
   int tx, ty, tz; // stored kernel extents
   int parT;
   int nrhs;
+  int zmir;  // fused z pass: one kernel load per mirror pair of z frequencies
   double scale;
   FDiv md;    // division by the tile width TX
   FDiv nind;  // division by nin
@@ -737,6 +738,28 @@ constexpr int zf_min_blocks(int T) { return 65536 / (T * 128) > 1 ? 65536 / (T *
 // does not fit 128 FP64 registers, so those lengths keep the unfused kernel
 constexpr bool zf_ok(int CS, int P) { return CS == 8 || ct_radix(P, ct_nst(P) - 1) <= 4; }
 
+// the 3x3 symmetric multiply of one frequency with stored kernel values g
+// (xx, yy, zz, xy, xz, yz), off-diagonal signs by the mirror flags, scaled
+template <typename C>
+__device__ __forceinline__ void zmul3(C& x0, C& x1, C& x2, const C (&g)[6], int rx, int ry, int rz,
+                                      typename Real<C>::T s) {
+  using Tr = typename Real<C>::T;
+  const C gxy = cscale(g[3], (rx ^ ry) ? (Tr)-1 : (Tr)1);
+  const C gxz = cscale(g[4], (rx ^ rz) ? (Tr)-1 : (Tr)1);
+  const C gyz = cscale(g[5], (ry ^ rz) ? (Tr)-1 : (Tr)1);
+  const C a = x0, b = x1, c = x2;
+  x0 = cscale(cadd(cadd(cmul(g[0], a), cmul(gxy, b)), cmul(gxz, c)), s);
+  x1 = cscale(cadd(cadd(cmul(gxy, a), cmul(g[1], b)), cmul(gyz, c)), s);
+  x2 = cscale(cadd(cadd(cmul(gxz, a), cmul(gyz, b)), cmul(g[2], c)), s);
+}
+
+// Lengths whose fused stage can hold two tasks' values (3 * 2 * RL per
+// thread): the mirror-pair form of k_zf_ct
+template <typename C, int P>
+constexpr bool zm_ok() {
+  return ct_radix(P, ct_nst(P) - 1) <= 2 && (P / ct_radix(P, ct_nst(P) - 1)) % 2 == 0;
+}
+
 template <typename C, int P, int TX>
 __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX, P))) k_zf_ct(const ZParams<C> p) {
   using Tr = typename Real<C>::T;
@@ -785,56 +808,124 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
   const int tx = p.tx, ty = p.ty, tz = p.tz;
   const Tr s = (Tr)p.scale;
   const C* const tw = p.tw;
+  bool paired = false;
+  if constexpr (zm_ok<C, P>()) {
+    if (p.zmir && !p.ax[2].full) {
+      // Mirror pairs: frequency j + r*TPL (this task's r-th value) and
+      // P - j - r*TPL = (TPL - j) + (RL-1-r)*TPL (task TPL - j, value
+      // RL-1-r) read the same stored kernel entry with mirrored signs, so
+      // one thread takes both tasks and loads each entry once.  Task pair
+      // (0, TPL/2) holds two self-mirrored sets and loads for both.  The
+      // arithmetic per frequency is the single-task form's.
+      constexpr int NPT = TX * (TPL / 2);
+      constexpr int K2 = (NPT + T - 1) / T;
 #pragma unroll
-  for (int k = 0; k < K; ++k) {
-    const int task = (int)threadIdx.x + k * T;
-    if (NTASK % T != 0 && task >= NTASK) continue;
-    const int l = task % TX, j = task / TX;
-    if (l >= tmax) continue;  // columns past Px are never stored
-    C v[3][RL];
+      for (int k = 0; k < K2; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        if (NPT % T != 0 && task >= NPT) continue;
+        const int l = task % TX, jp = task / TX;
+        if (l >= tmax) continue;  // columns past Px are never stored
+        const int jj[2] = {jp, jp ? TPL - jp : TPL / 2};
+        C v[2][3][RL];
 #pragma unroll
-    for (int c = 0; c < 3; ++c)
+        for (int h = 0; h < 2; ++h) {
 #pragma unroll
-      for (int r = 0; r < RL; ++r) v[c][r] = sm[c * CH + (j + r * TPL) * TX + l];
-    // forward last stage (span TPL: twiddle exponent r * j)
-    {
-      C w[RL];
-      twiddles<RL, false>(tw, j, w);
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) v[h][c][r] = sm[c * CH + (jj[h] + r * TPL) * TX + l];
+          C w[RL];
+          twiddles<RL, false>(tw, jj[h], w);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int r = 1; r < RL; ++r) v[h][c][r] = cmul(v[h][c][r], w[r]);
+            Bfly<RL, false, C>::run(v[h][c], tw, TPL);
+          }
+        }
+        int px, ix, rx;
+        ax_map(p.ax[0], kx0 + l, px, ix, rx);
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int f0 = jj[0] + r * TPL, f1 = jj[1] + (RL - 1 - r) * TPL;
+          int pz0, iz0, rz0, pz1, iz1, rz1;
+          ax_map(p.ax[2], f0, pz0, iz0, rz0);
+          ax_map(p.ax[2], f1, pz1, iz1, rz1);
+          C g[6];
+          const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz0, iz0, iy, ix, tx, ty, tz);
+#pragma unroll
+          for (int q = 0; q < 6; ++q) g[q] = ker_ld(gp, q, tx);
+          zmul3(v[0][0][r], v[0][1][r], v[0][2][r], g, rx, ry, rz0, s);
+          if (pz1 != pz0 || iz1 != iz0) {
+            gp = ker_at(p.ker, 4 * px + 2 * py + pz1, iz1, iy, ix, tx, ty, tz);
+#pragma unroll
+            for (int q = 0; q < 6; ++q) g[q] = ker_ld(gp, q, tx);
+          }
+          zmul3(v[1][0][RL - 1 - r], v[1][1][RL - 1 - r], v[1][2][RL - 1 - r], g, rx, ry, rz1, s);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Bfly<RL, true, C>::run(v[h][c], tw, TPL);
+#pragma unroll
+            for (int r = 0; r < RL; ++r) sm[c * CH + (jj[h] + r * TPL) * TX + l] = v[h][c][r];
+          }
+      }
+      paired = true;
+    }
+  }
+  if (!paired) {
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NTASK % T != 0 && task >= NTASK) continue;
+      const int l = task % TX, j = task / TX;
+      if (l >= tmax) continue;  // columns past Px are never stored
+      C v[3][RL];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) v[c][r] = sm[c * CH + (j + r * TPL) * TX + l];
+      // forward last stage (span TPL: twiddle exponent r * j)
+      {
+        C w[RL];
+        twiddles<RL, false>(tw, j, w);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int r = 1; r < RL; ++r) v[c][r] = cmul(v[c][r], w[r]);
+          Bfly<RL, false, C>::run(v[c], tw, TPL);
+        }
+      }
+      // v[c][r] is frequency kz = j + r * TPL: 3x3 symmetric multiply with the
+      // stored kernel (mirror / sign rules of mulBrnDev!)
+      int px, ix, rx;
+      ax_map(p.ax[0], kx0 + l, px, ix, rx);
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        const int kz = j + r * TPL;
+        int pz, iz, rz;
+        ax_map(p.ax[2], kz, pz, iz, rz);
+        const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
+        const C gxx = ker_ld(gp, 0, tx), gyy = ker_ld(gp, 1, tx), gzz = ker_ld(gp, 2, tx);
+        const C gxy = cscale(ker_ld(gp, 3, tx), (rx ^ ry) ? (Tr)-1 : (Tr)1);
+        const C gxz = cscale(ker_ld(gp, 4, tx), (rx ^ rz) ? (Tr)-1 : (Tr)1);
+        const C gyz = cscale(ker_ld(gp, 5, tx), (ry ^ rz) ? (Tr)-1 : (Tr)1);
+        const C x0 = v[0][r], x1 = v[1][r], x2 = v[2][r];
+        v[0][r] = cscale(cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2)), s);
+        v[1][r] = cscale(cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2)), s);
+        v[2][r] = cscale(cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2)), s);
+      }
+      // inverse first stage (span 1: no twiddles).  Its output of natural
+      // index j * RL + r goes back to the slot the thread read, j + r * TPL,
+      // so no thread overwrites a value another one has not read yet; the next
+      // stage reads through that permutation.
 #pragma unroll
       for (int c = 0; c < 3; ++c) {
+        Bfly<RL, true, C>::run(v[c], tw, TPL);
 #pragma unroll
-        for (int r = 1; r < RL; ++r) v[c][r] = cmul(v[c][r], w[r]);
-        Bfly<RL, false, C>::run(v[c], tw, TPL);
+        for (int r = 0; r < RL; ++r) sm[c * CH + (j + r * TPL) * TX + l] = v[c][r];
       }
-    }
-    // v[c][r] is frequency kz = j + r * TPL: 3x3 symmetric multiply with the
-    // stored kernel (mirror / sign rules of mulBrnDev!)
-    int px, ix, rx;
-    ax_map(p.ax[0], kx0 + l, px, ix, rx);
-#pragma unroll
-    for (int r = 0; r < RL; ++r) {
-      const int kz = j + r * TPL;
-      int pz, iz, rz;
-      ax_map(p.ax[2], kz, pz, iz, rz);
-      const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
-      const C gxx = ker_ld(gp, 0, tx), gyy = ker_ld(gp, 1, tx), gzz = ker_ld(gp, 2, tx);
-      const C gxy = cscale(ker_ld(gp, 3, tx), (rx ^ ry) ? (Tr)-1 : (Tr)1);
-      const C gxz = cscale(ker_ld(gp, 4, tx), (rx ^ rz) ? (Tr)-1 : (Tr)1);
-      const C gyz = cscale(ker_ld(gp, 5, tx), (ry ^ rz) ? (Tr)-1 : (Tr)1);
-      const C x0 = v[0][r], x1 = v[1][r], x2 = v[2][r];
-      v[0][r] = cscale(cadd(cadd(cmul(gxx, x0), cmul(gxy, x1)), cmul(gxz, x2)), s);
-      v[1][r] = cscale(cadd(cadd(cmul(gxy, x0), cmul(gyy, x1)), cmul(gyz, x2)), s);
-      v[2][r] = cscale(cadd(cadd(cmul(gxz, x0), cmul(gyz, x1)), cmul(gzz, x2)), s);
-    }
-    // inverse first stage (span 1: no twiddles).  Its output of natural
-    // index j * RL + r goes back to the slot the thread read, j + r * TPL,
-    // so no thread overwrites a value another one has not read yet; the next
-    // stage reads through that permutation.
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      Bfly<RL, true, C>::run(v[c], tw, TPL);
-#pragma unroll
-      for (int r = 0; r < RL; ++r) sm[c * CH + (j + r * TPL) * TX + l] = v[c][r];
     }
   }
   __syncthreads();
@@ -1252,6 +1343,15 @@ static inline bool ztwo() {
   }();
   return on;
 }
+// mirror-pair tasks in the fused z pass where the launch shape asks for
+// them (GILA_ZMIRROR=0: never, 2: always); read at every launch, results
+// are identical either way
+static inline int zmirror(int want) {
+  const char* e = getenv("GILA_ZMIRROR");
+  if (e && e[0] == '0') return 0;
+  if (e && e[0] == '2') return 1;
+  return want != 0;
+}
 static inline bool zpair() {
   static const bool on = [] {
     const char* e = getenv("GILA_ZPAIR");
@@ -1475,6 +1575,7 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
   p.tz = g.tru[2];
   p.parT = g.parT;
   p.nrhs = nrhs;
+  p.zmir = zmirror(L.z_mir);
   p.scale = d.scale;
   for (int k = 0; k < 3; ++k) {
     p.ax[k].brn = g.P[k] / 2;

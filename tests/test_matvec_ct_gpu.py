@@ -104,3 +104,25 @@ def test_ct_radix_orders(case, dtype):
             assert rel_l2(gila.egoOpr(mem, x), y_ref) <= tol
     with pytest.raises(gila.GilaError):
         mem.schedule = (2, 0)
+
+
+@pytest.mark.parametrize("case", [CT_CASES[1], CT_CASES[2], CT_CASES[10], ((64, 64, 64), None, (0, 0, 0))],
+                         ids=lambda c: f"{c[0]}<-{c[1]}")
+def test_ct_z_mirror_pairs(case, monkeypatch):
+    """The fused z pass with one task per mirror pair of z frequencies (one
+    kernel load for kz and P - kz) against one task per frequency, at every
+    z tile: the same arithmetic, so bit-identical, and both on the oracle."""
+    gila = load_pkg()
+    mix, mem, ref = _build(gila, case, np.complex128)
+    x = np.asfortranarray(seeded_current(mix.src_cel, 29).astype(np.complex128))
+    y_ref = ego_opr(ref, x.astype(np.complex128))
+    for z in (4, 8, 16):
+        mem.tiles = (0, 0, 0, z)
+        if mem.tiles[3] != z:
+            continue
+        outs = []
+        for mode in ("0", "2"):
+            monkeypatch.setenv("GILA_ZMIRROR", mode)
+            outs.append(gila.egoOpr(mem, x))
+        assert rel_l2(outs[1], y_ref) <= TOL_F64
+        assert np.array_equal(outs[0], outs[1])
