@@ -166,8 +166,9 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
 
 /* Launch shapes.  tiles = {x-forward lines per CTA, x-inverse lines per CTA,
  * y-pass kx tile, z-pass kx tile}.  No counterpart in the reference.  The
- * first apply of an operator picks the y and z tiles (and the radix order of
- * the x and y transforms, gila_opr_get_schedule) by timing every compiled
+ * first apply of an operator picks the y and z tiles (with the radix order of
+ * the x and y transforms, gila_opr_get_schedule, and the task form of the
+ * fused z pass: one task per frequency or per mirror pair) by timing every compiled
  * candidate on the operator's workspaces (cached per context and geometry;
  * GILA_AUTOTUNE=0 keeps the defaults); gila_opr_autotune re-runs that for a
  * batch of nrhs vectors; gila_opr_set_tiles forces tiles (entries <= 0 or
