@@ -87,7 +87,8 @@ def test_ct_multi_rhs(dtype, case):
         assert np.array_equal(Y[..., k], gila.egoOpr(mem, xs[k]))
 
 
-@pytest.mark.parametrize("case", [CT_CASES[1], CT_CASES[2], CT_CASES[6]], ids=lambda c: f"{c[0]}<-{c[1]}")
+@pytest.mark.parametrize("case", [CT_CASES[1], CT_CASES[2], CT_CASES[6], CT_CASES[7], CT_CASES[14], CT_CASES[15],
+                                  CT_CASES[8]], ids=lambda c: f"{c[0]}<-{c[1]}")
 @pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
 def test_ct_radix_orders(case, dtype):
     """Both radix orders of the x and y transforms (greedy, reversed): the
