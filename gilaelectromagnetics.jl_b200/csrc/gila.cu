@@ -3,6 +3,7 @@
 // the apply mirrors egoOpr! (src/glaAct.jl:33-49) and mul! (src/glaLinAlg.jl).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -495,7 +496,7 @@ static bool tune_debug() {
 // workspaces A and B laid out for g, all on stream s.
 template <typename C>
 static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C* dout, C* A, C* B,
-                           cudaStream_t s, Launch& best) {
+                           cudaStream_t s, Launch& best, const Launch* keep_radix = nullptr) {
   cudaError_t e = cudaSuccess;
   cudaEvent_t ev[2];
   GILA_CUDA_TRY(cudaEventCreate(&ev[0]));
@@ -528,6 +529,10 @@ static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C
   };
   const int cs = (int)csize(c.dtype);
   best = default_launch(c);
+  if (keep_radix) {
+    best.x_rev = keep_radix->x_rev;
+    best.y_rev = keep_radix->y_rev;
+  }
   std::vector<int> zc = ct_tiles(cs, c.geom.P[2], true), yc = ct_tiles(cs, c.geom.P[1], false);
   // z tile width jointly with the task form of the fused z pass (one task
   // per thread slot, or one per mirror pair of z frequencies where the
@@ -572,7 +577,7 @@ static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C
   // radix order of the x and y passes: the greedy one (radix-8 stages first)
   // or its reverse, where they differ (specialised lengths, radix list not a
   // palindrome); phases 0 and 2 hold both passes
-  for (int ax = 0; ax < 2 && e == cudaSuccess; ++ax) {
+  for (int ax = 0; ax < 2 && e == cudaSuccess && !keep_radix; ++ax) {
     const AxisPlan& pl = c.plan[ax];
     bool pal = true;
     for (int k = 0; k < pl.nst; ++k) pal = pal && pl.radix[k] == pl.radix[pl.nst - 1 - k];
@@ -601,7 +606,7 @@ static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C
 
 // the operator's own workspaces and two scratch vectors
 template <typename C>
-static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
+static gila_status tune_t(Core& c, int64_t nrhs, Launch& best, const Launch* keep_radix) {
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
   C *din = nullptr, *dout = nullptr;
   GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
@@ -613,7 +618,7 @@ static gila_status tune_t(Core& c, int64_t nrhs, Launch& best) {
     return cuda_fail(e, "autotune buffers");
   }
   const gila_status s =
-      tune_on<C>(c, c.geom, nrhs, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B), c.stream, best);
+      tune_on<C>(c, c.geom, nrhs, din, dout, static_cast<C*>(c.A), static_cast<C*>(c.B), c.stream, best, keep_radix);
   cudaStreamSynchronize(c.stream);
   cudaFree(din);
   cudaFree(dout);
@@ -651,41 +656,76 @@ template gila_status tuned_launch<double2>(Core&, const Geom&, int64_t, const do
 template gila_status tuned_launch<float2>(Core&, const Geom&, int64_t, const float2*, float2*, float2*, float2*,
                                           cudaStream_t, Launch&);
 
-gila_status autotune(Core& c, int64_t nrhs) {
-  gila_status s = ensure_work(c, nrhs);
+// Batch size a tuning run times: nrhs, capped so that its two scratch
+// vector sets stay within 512 MiB (beyond that the grids are large and the
+// choice no longer moves).
+static int64_t tune_rhs(const Core& c, int64_t nrhs) {
+  const int64_t per = (in_elems(c) + out_elems(c)) * (int64_t)csize(c.dtype);
+  const int64_t cap = std::max<int64_t>(1, (512LL << 20) / std::max<int64_t>(per, 1));
+  return std::min(nrhs, cap);
+}
+
+// Cache key of a tuning run; a run that kept the operator's radix schedule
+// (re-tuning for another batch size) records that schedule too.
+static std::string tune_key_of(const Core& c, int64_t nb, const Launch* keep_radix) {
+  std::string k = tune_key(c, nb);
+  if (keep_radix) k += "|r" + std::to_string(keep_radix->x_rev) + std::to_string(keep_radix->y_rev);
+  return k;
+}
+
+// A tuning run for nrhs vectors.  The operator's first run picks every
+// launch choice; later runs for other batch sizes keep its radix schedule,
+// the one choice that changes rounding, so that an operator's result for a
+// vector never depends on the batch it came in.
+static gila_status autotune_run(Core& c, int64_t nrhs, const Launch* keep_radix) {
+  const int64_t nb = tune_rhs(c, nrhs);
+  gila_status s = ensure_work(c, nb);
   if (s != GILA_OK) return s;
   Launch L;
   if (c.dtype == GILA_C128)
-    s = tune_t<double2>(c, nrhs, L);
+    s = tune_t<double2>(c, nb, L, keep_radix);
   else
-    s = tune_t<float2>(c, nrhs, L);
+    s = tune_t<float2>(c, nb, L, keep_radix);
   if (s != GILA_OK) return s;
   c.launch = L;
   c.tuned = true;
+  c.tuned_rhs = nrhs;
   std::lock_guard<std::mutex> lk(c.ctx->mu);
-  c.ctx->tune_cache[tune_key(c, nrhs)] = L;
+  c.ctx->tune_cache[tune_key_of(c, nb, keep_radix)] = L;
   return GILA_OK;
 }
 
-// The launch shapes of the first use: the context's cached choice for this
-// geometry, else a tuning run (GILA_AUTOTUNE=0: the defaults).
+gila_status autotune(Core& c, int64_t nrhs) {
+  const Launch keep = c.launch;
+  return autotune_run(c, nrhs, c.tuned ? &keep : nullptr);
+}
+
+// The launch shapes for a batch of nrhs vectors: those already in use when
+// they were picked for this batch size (or forced by the caller), else the
+// context's cached choice, else a tuning run (GILA_AUTOTUNE=0: the
+// defaults).  Tile widths and the z task form are re-picked per batch size;
+// the radix schedule stays the operator's first choice.
 gila_status ensure_tuned(Core& c, int64_t nrhs) {
-  if (c.tuned) return GILA_OK;
+  if (c.tuned && (c.pinned || c.tuned_rhs == nrhs)) return GILA_OK;
+  if (autotune_off()) {
+    if (!c.tuned) c.launch = default_launch(c);
+    c.tuned = true;
+    c.tuned_rhs = nrhs;
+    return GILA_OK;
+  }
+  const Launch keep = c.launch;
+  const Launch* kr = c.tuned ? &keep : nullptr;
   {
     std::lock_guard<std::mutex> lk(c.ctx->mu);
-    auto it = c.ctx->tune_cache.find(tune_key(c, nrhs));
+    auto it = c.ctx->tune_cache.find(tune_key_of(c, tune_rhs(c, nrhs), kr));
     if (it != c.ctx->tune_cache.end()) {
       c.launch = it->second;
       c.tuned = true;
+      c.tuned_rhs = nrhs;
       return GILA_OK;
     }
   }
-  if (autotune_off()) {
-    c.launch = default_launch(c);
-    c.tuned = true;
-    return GILA_OK;
-  }
-  return autotune(c, nrhs);
+  return autotune_run(c, nrhs, kr);
 }
 
 // staging buffer of at least n elements (contents not kept)
@@ -1093,6 +1133,7 @@ gila_status gila_opr_autotune(gila_opr* opr, int64_t nrhs, int32_t tiles[4]) {
   Core& c = *opr->core;
   std::lock_guard<std::mutex> lk(c.mu);
   GILA_CUDA_TRY(cudaSetDevice(c.device));
+  c.pinned = false;
   gila_status s = autotune(c, nrhs);
   if (s != GILA_OK) return s;
   if (tiles) {
@@ -1126,6 +1167,7 @@ gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]) {
   if (tiles[3] > 0) L.z_tx = ct_tile_pick(cs, c.geom.P[2], tiles[3], true) == tiles[3] ? tiles[3] : L.z_tx;
   c.launch = L;
   c.tuned = true;
+  c.pinned = true;
   return GILA_OK;
 }
 
@@ -1149,6 +1191,7 @@ gila_status gila_opr_set_schedule(gila_opr* opr, const int32_t sched[2]) {
   if (sched[1] >= 0) L.y_rev = sched[1];
   c.launch = L;
   c.tuned = true;
+  c.pinned = true;
   return GILA_OK;
 }
 

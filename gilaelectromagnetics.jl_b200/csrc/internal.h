@@ -82,6 +82,8 @@ struct Core {
   cudaEvent_t ev_out_ready[2] = {nullptr, nullptr}, ev_out_free[2] = {nullptr, nullptr};
   Launch launch{};
   bool tuned = false;
+  int64_t tuned_rhs = 0;  // batch size c.launch was picked for
+  bool pinned = false;    // launch shapes forced by the caller (set_tiles / set_schedule)
   cudaStream_t stream = nullptr;
   std::mutex mu;
   // a solve batch kept resident between gila_ls_solve calls (opts->keep)

@@ -127,3 +127,33 @@ def test_ct_z_mirror_pairs(case, monkeypatch):
             outs.append(gila.egoOpr(mem, x))
         assert rel_l2(outs[1], y_ref) <= TOL_F64
         assert np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_ct_batch_sizes_keep_results(dtype):
+    """Launch shapes are re-picked per batch size of device-resident
+    vectors, the radix schedule is not: an operator first used on one
+    vector, then on batches of 4 and 2, keeps its schedule and gives every
+    vector bit-identical results."""
+    import torch
+
+    gila = load_pkg()
+    mix, mem, ref = _build(gila, CT_CASES[1], dtype)
+    n = mix.src_cel
+    xs = [np.asfortranarray(seeded_current(n, 40 + k).astype(dtype)) for k in range(4)]
+    xd = torch.stack([torch.from_numpy(x.ravel(order="F").copy()).reshape(3, n[2], n[1], n[0]) for x in xs]).cuda()
+    singles = []
+    for k in range(4):
+        y = torch.empty_like(xd[k])
+        mem.apply_into(xd[k], y)
+        singles.append(y)
+    sched = mem.schedule
+    for nb in (4, 2):
+        Y = torch.empty_like(xd[:nb])
+        mem.apply_into(xd[:nb].contiguous(), Y, nrhs=nb)
+        assert mem.schedule == sched
+        for k in range(nb):
+            assert torch.equal(Y[k], singles[k])
+    y0 = singles[0].cpu().numpy().reshape(-1)
+    y_ref = ego_opr(ref, xs[0].astype(np.complex128)).ravel(order="F")
+    assert rel_l2(y0, y_ref) <= (TOL_F64 if dtype == np.complex128 else TOL_F32)
