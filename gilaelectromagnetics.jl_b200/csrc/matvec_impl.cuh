@@ -1120,8 +1120,16 @@ __global__ void __launch_bounds__(zr_threads(TX, P), zr_min_blocks(zr_threads(TX
 #ifndef GILA_ZF2_CAP
 #define GILA_ZF2_CAP 1
 #endif
+// CTAs per SM the FP32 fused z kernel is compiled for: registers capped at
+// 128 per thread, or at 168 where the fused stage is radix 3 (P = 96, 192,
+// 384; measured z pass at P = 96, 96x96x48 cells: 0.0675 -> 0.0606 ms,
+// unchanged at 192; at P = 256 the higher cap measured 16% slower)
+constexpr int zf2_min_blocks(int T, int P) {
+  const int regs = ct_radix(P, ct_nst(P) - 1) == 3 ? 168 : 128;
+  return 65536 / (T * regs) > 1 ? 65536 / (T * regs) : 1;
+}
 template <int P, int TX>
-__global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf_min_blocks(ct_threads2(TX, P)) : 1)
+__global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf2_min_blocks(ct_threads2(TX, P), P) : 1)
     k_zf2_ct(const ZParams<float2> p) {
   using C = float2;
   constexpr int T = ct_threads2(TX, P);
