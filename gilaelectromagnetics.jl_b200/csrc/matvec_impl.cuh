@@ -410,6 +410,16 @@ __global__ void __launch_bounds__(512) k_xinv(const XiParams<C> p) {
 // The same five passes with the transform length P, tile width and thread
 // count as template constants (see fft_ct.cuh).
 
+// CTAs per SM a pass kernel is compiled for: at power-of-two lengths,
+// registers capped at 48 per thread (y passes: 0.4131 -> 0.4107 ms per
+// matvec at 128x128x64 F64, 3.470 -> 3.439 ms at 256x256x128,
+// bit-identical); lengths with a radix-3 stage would spill 300+ bytes at
+// that cap and keep no hint
+constexpr int pow2_min_blocks(int T, int P) {
+  const int b = ct_odd(P) == 1 ? 65536 / (T * 48) : 1;
+  return b < 1 ? 1 : (b > 32 ? 32 : b);  // at most 32 resident CTAs per SM
+}
+
 template <typename C, int P, bool REV>
 __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xfwd_ct(const XfParams<C> p) {
   constexpr int M = ct_xlines<sizeof(C)>(P);
@@ -537,7 +547,7 @@ __global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xinv2_ct(c
 }
 
 template <typename C, int P, bool INV, int TX, bool REV>
-__global__ void __launch_bounds__(ct_threads(TX, P)) k_y_ct(const YParams<C> p) {
+__global__ void __launch_bounds__(ct_threads(TX, P), pow2_min_blocks(ct_threads(TX, P), P)) k_y_ct(const YParams<C> p) {
   constexpr int T = ct_threads(TX, P);
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* const sm = reinterpret_cast<C*>(smem_raw);
