@@ -170,10 +170,12 @@ gila_status gila_opr_time_passes(gila_opr* opr, int64_t nrhs, int reps, double m
  * the x and y transforms, gila_opr_get_schedule, and the task form of the
  * fused z pass: one task per frequency or per mirror pair) by timing every compiled
  * candidate on the operator's workspaces (cached per context and geometry;
- * GILA_AUTOTUNE=0 keeps the defaults); gila_opr_autotune re-runs that for a
- * batch of nrhs vectors; gila_opr_set_tiles forces tiles (entries <= 0 or
- * not compiled for the transform length are ignored).  Tiles never change
- * results, only speed. */
+ * GILA_AUTOTUNE=0 keeps the defaults).  An apply with another number of
+ * device-resident vectors re-times the tiles and the task form for that
+ * count and keeps the radix order.  gila_opr_autotune re-runs the timing for
+ * a batch of nrhs vectors; gila_opr_set_tiles forces tiles (entries <= 0 or
+ * not compiled for the transform length are ignored) for every batch size.
+ * Tiles never change results, only speed. */
 gila_status gila_opr_autotune(gila_opr* opr, int64_t nrhs, int32_t tiles[4]);
 gila_status gila_opr_get_tiles(gila_opr* opr, int32_t tiles[4]);
 gila_status gila_opr_set_tiles(gila_opr* opr, const int32_t tiles[4]);
