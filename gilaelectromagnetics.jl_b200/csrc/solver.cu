@@ -727,8 +727,16 @@ class LsBatchT final : public LsBatch {
     // widths and radix orders that win for one vector need not win for a
     // chunk of several.  Timed on zero vectors (G 0 = 0 leaves every
     // buffer finite), or the operators' own single-vector choice.
-    op64_.launch = g64_.launch;
-    opi_.launch = gi_.launch;
+    {  // another thread's apply may be re-picking an operator's shapes
+      std::lock_guard<std::mutex> lk(g64_.mu);
+      op64_.launch = g64_.launch;
+    }
+    if (&gi_ == &g64_) {
+      opi_.launch = op64_.launch;
+    } else {
+      std::lock_guard<std::mutex> lk(gi_.mu);
+      opi_.launch = gi_.launch;
+    }
     if (cfg_.tune) {
       gila_status st;
       GILA_CUDA_TRY(cudaMemsetAsync(x64_, 0, vb * sizeof(double2), s_));
