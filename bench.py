@@ -4,14 +4,15 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
 
 One step = one application of the ComplexF64 self Green operator to one
-source current on the 128x128x64-cell volume with 1/32-wavelength cells (the
-matvec precision sweep configuration; its ComplexF32 leg, the external
-64^3 -> 64x64x32 operator and the 256x256x128 roofline target are reported
-in "sweep").  Inputs are seeded i.i.d. complex N(0,1) currents and a seeded
-synthetic Fourier kernel with the reference's storage shapes (kernel values do
-not change the matvec's work).  Under torchrun each rank runs an independent
-replica on its own GPU (weak scaling); `value` is the whole-job matvec/s from
-the max over ranks of the device time.
+source current on the 256x256x128-cell volume with 1/32-wavelength cells (the
+largest single-GPU configuration, the thin-film volume; its ComplexF32 leg,
+the 128x128x64 self and 64^3 -> 64x64x32 external operators of the matvec
+precision sweep are reported in "sweep").  Inputs are seeded i.i.d. complex
+N(0,1) currents and a seeded synthetic Fourier kernel with the reference's
+storage shapes (kernel values do not change the matvec's work).  Under
+torchrun each rank runs an independent replica on its own GPU (weak
+scaling); `value` is the whole-job matvec/s from the max over ranks of the
+device time.
 
 Prints one JSON line (rank 0).
 """
@@ -35,11 +36,21 @@ PKG = os.path.join(ROOT, "gilaelectromagnetics.jl_b200")
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-METRIC = "Green matvec/s (ComplexF64 egoOpr!, self 128x128x64)"
-CEL = (128, 128, 64)
+METRIC = "Green matvec/s (ComplexF64 egoOpr!, self 256x256x128)"
+CEL = (256, 256, 128)
+SWEEP_CEL = (128, 128, 64)
 SCL = ("1/32", "1/32", "1/32")
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-E2E_BATCH = 20  # host vectors per API call in the end-to-end leg
+E2E_BATCH = 4  # host vectors (403 MB each) per API call in the end-to-end leg
+
+
+def bench_config(c64: bool, world: int) -> dict:
+    """The `config` of the bench line; both arms print the same dict."""
+    return {"workload": "self Green operator 256x256x128 cells, 1/32 wavelength, "
+                        + ("ComplexF32" if c64 else "ComplexF64") + ", 1 vector/step",
+            "parallelism": f"replicas x{world}",
+            "l2": "flushed (256 MB write) between timed steps; each step's vectors (403 MB in, 403 MB out) "
+                  "are larger than the 126 MB L2"}
 
 
 def load_pkg():
@@ -249,10 +260,10 @@ def main():
                          "short mixed-precision solves on 96x96x48, 'build' = the GPU kernel build of a 32^3 "
                          "self operator, 'matvec256' = 4 matvecs of the 256x256x128 self operator in the "
                          "precision of --dtype; prints no bench line")
-    ap.add_argument("--serve-burst", type=int, default=200,
-                    help="requests of the burst that measures saturation (at most --serve-requests)")
-    ap.add_argument("--serve-requests", type=int, default=40,
-                    help="requests of the Poisson stream and of the burst that measures saturation")
+    ap.add_argument("--serve-requests", type=int, default=2000,
+                    help="requests of the Poisson stream of the serving leg")
+    ap.add_argument("--serve-closed-s", type=float, default=60.0,
+                    help="seconds of the closed loop that measures the serving saturation rate")
     a = ap.parse_args()
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -325,7 +336,7 @@ def main():
     zb = zpass_bytes(CEL, CEL, tru, cs)
     peak, peak_kind = measured_peak()
     achieved = zb / (passes[1] / 1e3) / 1e9
-    traffic = ncu_traffic(f"z_pass_{a.dtype}_128x128x64")
+    traffic = ncu_traffic(f"z_pass_{a.dtype}_256x256x128")
     roofline = {"bound": "hbm",
                 "kernel": ("k_zf2_ct" if f32 else "k_zf_ct") + " (z pencils: forward FFT, 3x3 multiply fused with "
                           "the last / first butterflies, inverse FFT)",
@@ -342,11 +353,10 @@ def main():
         "warmup": W, "ms_per_step": round(ms_max / a.steps, 4), "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32" if f32 else "f64",
         "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
-        "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
-                               + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
-                   "parallelism": f"replicas x{world}", "l2": "flushed (256 MB write) between timed steps"},
+        "config": bench_config(f32, world),
         "e2e": {"value": round(e2e_value, 2), "unit": "matvec/s", "h2d_bytes_per_step": nbytes,
-                "d2h_bytes_per_step": nbytes, "api": "GlaOprMem.apply_into with pinned host tensors, 20 vectors per call (copies overlap the passes)",
+                "d2h_bytes_per_step": nbytes,
+                "api": f"GlaOprMem.apply_into with pinned host tensors, {kb} vectors per call (copies overlap the passes)",
                 "copy_bound": copy_bound, "frac_of_copy_bound": round(e2e_value / world / copy_bound["vectors_per_s"], 4)},
         "gpu_launches": int(mem.launches_per_apply(1)) * a.steps,
         "roofline": roofline,
@@ -357,11 +367,11 @@ def main():
         out["cpu_baseline"], xo, yo = cpu_baseline()
         out["oracle_check"] = oracle_check(gila, xo, yo)
     if not a.no_sweep and world == 1:
-        out["sweep"] = sweep(torch, gila, stream, flush, y_dev)
+        out["sweep"] = sweep(torch, gila, stream, flush)
     if not a.no_solve and world == 1:
         out["solve"] = solve_bench(torch, gila)
     if not a.no_serve and world == 1:
-        out["serve"] = serve_bench(gila, a.serve_requests, a.serve_burst)
+        out["serve"] = serve_bench(gila, a.serve_requests, a.serve_closed_s)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -370,18 +380,26 @@ def main():
     return 0
 
 
-def sweep(torch, gila, stream, flush, y64):
-    """F32 leg, external operator and the 256x256x128 roofline target."""
+def sweep(torch, gila, stream, flush):
+    """The ComplexF32 leg of the bench workload and the matvec precision sweep
+    configuration: self 128x128x64 (ComplexF64 and ComplexF32, one and four
+    vectors per apply) and external 64^3 -> 64x64x32 offset 80 cells along x."""
     res = {}
     peak, _ = measured_peak()
-    # F32 self 128x128x64 and its error against the F64 GPU result
-    mem32, tru = make_opr(gila, CEL, np.complex64)
-    ms, _ = device_rate(torch, mem32, CEL, CEL, torch.complex64, 10, 3, stream, flush)
-    g = torch.Generator(device="cuda").manual_seed(3)
-    x64 = torch.randn((3, CEL[2], CEL[1], CEL[0]), dtype=torch.complex128, device="cuda", generator=g)
-    res["self_128x128x64_c64"] = {"ms": round(ms / 10, 4), "matvec_per_s": round(1e4 / ms, 2),
-                                  "tmin_frac": round(tmin_bytes(CEL, CEL, tru, 8) / (ms / 10 / 1e3) / 1e9 / peak, 4)}
-    del mem32
+    mem, tru = make_opr(gila, CEL, np.complex64)
+    ms, _ = device_rate(torch, mem, CEL, CEL, torch.complex64, 10, 3, stream, flush)
+    tm = tmin_bytes(CEL, CEL, tru, 8)
+    res["self_256x256x128_complex64"] = {"ms": round(ms / 10, 4), "matvec_per_s": round(1e4 / ms, 2), "tmin_bytes": tm,
+                                         "tmin_frac": round(tm / (ms / 10 / 1e3) / 1e9 / peak, 4)}
+    del mem
+    c = SWEEP_CEL
+    for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
+        mem, tru = make_opr(gila, c, dt)
+        ms, _ = device_rate(torch, mem, c, c, tdt, 20, 3, stream, flush)
+        res[f"self_128x128x64_{np.dtype(dt).name}"] = {
+            "ms": round(ms / 20, 4), "matvec_per_s": round(2e4 / ms, 2),
+            "tmin_frac": round(tmin_bytes(c, c, tru, cs) / (ms / 20 / 1e3) / 1e9 / peak, 4)}
+        del mem
     # external 64^3 -> 64x64x32, target offset 80 cells along x
     for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
         src, trg = (64, 64, 64), (64, 64, 32)
@@ -393,10 +411,10 @@ def sweep(torch, gila, stream, flush, y64):
         del mem
     # four vectors per apply (batched launches), per-vector time, L2 flushed between applies
     for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
-        mem, tru = make_opr(gila, CEL, dt)
+        mem, tru = make_opr(gila, c, dt)
         nb = 4
         g = torch.Generator(device="cuda").manual_seed(5)
-        xb = torch.randn((nb, 3, CEL[2], CEL[1], CEL[0]), dtype=tdt, device="cuda", generator=g)
+        xb = torch.randn((nb, 3, c[2], c[1], c[0]), dtype=tdt, device="cuda", generator=g)
         yb = torch.empty_like(xb)
         mem.autotune(nb)
         for _ in range(3):
@@ -413,18 +431,8 @@ def sweep(torch, gila, stream, flush, y64):
         ms = sum(a.elapsed_time(b) for a, b in evs) / (10 * nb)
         res[f"self_128x128x64_{np.dtype(dt).name}_4_per_apply"] = {
             "ms_per_vector": round(ms, 4), "matvec_per_s": round(1e3 / ms, 2),
-            "tmin_frac": round(tmin_bytes(CEL, CEL, tru, cs) / (ms / 1e3) / 1e9 / peak, 4)}
+            "tmin_frac": round(tmin_bytes(c, c, tru, cs) / (ms / 1e3) / 1e9 / peak, 4)}
         del mem, xb, yb
-    # 256x256x128 (north-star roofline target)
-    big = (256, 256, 128)
-    for dt, tdt, cs in ((np.complex128, torch.complex128, 16), (np.complex64, torch.complex64, 8)):
-        mem, tru = make_opr(gila, big, dt)
-        ms, _ = device_rate(torch, mem, big, big, tdt, 5, 3, stream, flush)
-        tm = tmin_bytes(big, big, tru, cs)
-        res[f"self_256x256x128_{np.dtype(dt).name}"] = {
-            "ms": round(ms / 5, 4), "matvec_per_s": round(5e3 / ms, 2), "tmin_bytes": tm,
-            "tmin_frac": round(tm / (ms / 5 / 1e3) / 1e9 / peak, 4)}
-        del mem
     torch.cuda.empty_cache()
     return res
 
@@ -605,43 +613,75 @@ def serve_request(cel, rng):
     return chi, b
 
 
-def serve_bench(gila, n_stream, n_burst=200):
+def serve_bench(gila, n_stream, closed_s=60.0, clients=40):
     """The request stream: solves of volumes drawn uniformly from
     SERVE_SHAPES (1/32-wavelength cells), each with its own medium and
     incident wave, tol 1e-6, ComplexF32 Krylov with FP64 reliable updates.
-    A burst of min(n_stream, n_burst) requests (submitted at once) measures
-    the saturation throughput; then n_stream requests drawn the same way arrive
-    as a Poisson process at 80% of it (seeded).
-    Inputs come from a pool of 3 seeded variants per shape."""
+
+    Saturation is the sustained completion rate of a closed loop: `clients`
+    requests are kept outstanding for `closed_s` seconds, each completion
+    immediately replaced by a new request of a uniformly drawn shape, so the
+    completed mix is the uniform mix and the rate is what the server sustains
+    on it (not a burst, which overstates a mixed stream's capacity).  Then
+    n_stream requests drawn the same way arrive as a Poisson process at 80%
+    of that rate (seeded); latency is submit -> solution in the caller's
+    buffer.  The queue (requests waiting for a slot) and the running count are
+    sampled every 0.5 s during the stream.  Inputs come from a pool of 3
+    seeded variants per shape."""
     rng = np.random.default_rng(11)
     pool = {c: [serve_request(c, rng) for _ in range(3)] for c in SERVE_SHAPES}
     srv = gila.SolveServer(slots=8, mixed=True)
-    res = {"shapes": ["x".join(map(str, c)) for c in SERVE_SHAPES], "tol": 1e-6}
+    key = lambda c: "x".join(map(str, c))  # noqa: E731
+    res = {"shapes": [key(c) for c in SERVE_SHAPES], "tol": 1e-6}
     try:
         # operators (built on the GPU) and one solve per shape, alone
         alone = {}
         for c in SERVE_SHAPES:
             t0 = time.perf_counter()
             _, inf, lat = srv.wait(srv.submit(c, SCL, *pool[c][0]))
-            alone["x".join(map(str, c))] = {"first_ms_incl_build": round((time.perf_counter() - t0) * 1e3, 1)}
+            alone[key(c)] = {"first_ms_incl_build": round((time.perf_counter() - t0) * 1e3, 1)}
             _, inf, lat = srv.wait(srv.submit(c, SCL, *pool[c][0]))
-            alone["x".join(map(str, c))].update({"ms": round(lat, 1), "cycles": inf.iters})
+            alone[key(c)].update({"ms": round(lat, 1), "cycles": inf.iters})
         res["alone"] = alone
-        # saturation: a burst
-        nb = max(4, min(n_stream, n_burst))
-        picks = [SERVE_SHAPES[i] for i in rng.integers(0, len(SERVE_SHAPES), nb)]
+        # saturation: closed loop of `clients` outstanding requests
+        t_stop = time.perf_counter() + closed_s
+        done_at, lock = [], threading.Lock()
+
+        def client(seed):
+            r = np.random.default_rng(seed)
+            while time.perf_counter() < t_stop:
+                c = SERVE_SHAPES[int(r.integers(0, len(SERVE_SHAPES)))]
+                srv.wait(srv.submit(c, SCL, *pool[c][int(r.integers(0, 3))]))
+                with lock:
+                    done_at.append(time.perf_counter())
+
         t0 = time.perf_counter()
-        tk = [srv.submit(c, SCL, *pool[c][int(rng.integers(0, 3))]) for c in picks]
-        for t in tk:
-            srv.wait(t)
-        sat = nb / (time.perf_counter() - t0)
-        res["saturation_solves_per_s"] = round(sat, 3)
+        th = [threading.Thread(target=client, args=(100 + i,)) for i in range(clients)]
+        for t in th:
+            t.start()
+        for t in th:
+            t.join()
+        in_window = [t for t in done_at if t <= t_stop]
+        sat = len(in_window) / (t_stop - t0)
+        res["saturation"] = {"solves_per_s": round(sat, 3), "completed_in_window": len(in_window),
+                             "window_s": round(t_stop - t0, 1), "outstanding": clients,
+                             "how": "closed loop, uniform shape per new request"}
         # Poisson stream at 80% of saturation
         lam = 0.8 * sat
         picks = [SERVE_SHAPES[i] for i in rng.integers(0, len(SERVE_SHAPES), n_stream)]
         gaps = rng.exponential(1.0 / lam, n_stream)
-        tk = []
+        samples, sampling = [], [True]
         t_start = time.perf_counter()
+
+        def sampler():
+            while sampling[0]:
+                st = srv.stats()
+                samples.append((round(time.perf_counter() - t_start, 2), st["queued"], st["running"]))
+                time.sleep(0.5)
+
+        sm = threading.Thread(target=sampler, daemon=True)
+        sm.start()
+        tk = []
         t_next = t_start
         for c, g in zip(picks, gaps):
             t_next += g
@@ -649,32 +689,46 @@ def serve_bench(gila, n_stream, n_burst=200):
             if d > 0:
                 time.sleep(d)
             tk.append((c, srv.submit(c, SCL, *pool[c][int(rng.integers(0, 3))])))
-        lats, conv = [], 0
-        per = {}
+        t_arrived = time.perf_counter() - t_start
+        lats, conv, per = [], 0, {}
         for c, t in tk:
             _, inf, lat = srv.wait(t)
             lats.append(lat)
             conv += inf.converged
-            per.setdefault("x".join(map(str, c)), []).append(lat)
+            per.setdefault(key(c), []).append(lat)
         wall = time.perf_counter() - t_start
+        sampling[0] = False
+        sm.join(timeout=2)
         lats = np.array(lats)
+        p99 = float(np.percentile(lats, 99))
+        tail = {}
+        for c, t in zip(picks, lats):
+            if t >= p99:
+                tail[key(c)] = tail.get(key(c), 0) + 1
+        step = max(1, len(samples) // 120)
+        q = [s_[1] for s_ in samples]
         res.update({
-            "requests": n_stream, "burst_requests": nb, "arrival_rate_per_s": round(lam, 3), "solves_per_s": round(n_stream / wall, 3),
-            "p50_ms": round(float(np.percentile(lats, 50)), 1), "p99_ms": round(float(np.percentile(lats, 99)), 1),
+            "requests": n_stream, "arrival_rate_per_s": round(lam, 3), "arrivals_s": round(t_arrived, 1),
+            "solves_per_s": round(n_stream / wall, 3),
+            "p50_ms": round(float(np.percentile(lats, 50)), 1), "p99_ms": round(p99, 1),
             "mean_ms": round(float(lats.mean()), 1), "converged": conv,
-            "p50_ms_by_shape": {k: round(float(np.median(v)), 1) for k, v in per.items()},
+            "by_shape": {k: {"n": len(v), "p50_ms": round(float(np.median(v)), 1),
+                             "p99_ms": round(float(np.percentile(v, 99)), 1)} for k, v in sorted(per.items())},
+            "p99_tail_shapes": tail,
+            "queue": {"max": max(q) if q else 0, "mean": round(float(np.mean(q)), 2) if q else 0,
+                      "last_third_mean": round(float(np.mean(q[2 * len(q) // 3:])), 2) if q else 0,
+                      "samples_t_queued_running": samples[::step]},
             "server": srv.stats()})
     finally:
         srv.close()
     return res
 
 
-def cpu_baseline():
-    """The oracle's restatement of the reference host path (egoBrnHst!) with
-    scipy.fft on all host threads, on the same configuration: a bounded
-    sample of 2 matvecs."""
+def _oracle_setup():
+    """The bench operator and input on the CPU oracle (restatement of
+    egoBrnHst!, scipy.fft on all host threads)."""
     from oracle.gla_mem import ExtInf, Vol
-    from oracle.matvec import OprMem, ego_opr, use_fft_workers
+    from oracle.matvec import OprMem, use_fft_workers
     n = os.cpu_count() or 1
     use_fft_workers(n)
     v = Vol.make(CEL, SCL)
@@ -682,31 +736,38 @@ def cpu_baseline():
     fur = synthetic_fur(tru_self(CEL), np.complex128, 1)
     rng = np.random.default_rng(3)
     x = rng.standard_normal((*CEL, 3)) + 1j * rng.standard_normal((*CEL, 3))
-    om = OprMem(mix, fur)
-    y = ego_opr(om, x)  # warm-up; its result checks the GPU matvecs
-    reps = 2
+    return OprMem(mix, fur), x, n
+
+
+def cpu_baseline():
+    """The oracle's restatement of the reference host path (egoBrnHst!) with
+    scipy.fft on all host threads, on the same configuration: a bounded
+    sample of one matvec (about 15-25 s of CPU work), whose result also
+    checks the GPU matvecs."""
+    from oracle.matvec import ego_opr
+    om, x, n = _oracle_setup()
     t0 = time.perf_counter()
-    for _ in range(reps):
-        ego_opr(om, x)
+    y = ego_opr(om, x)
     dt = time.perf_counter() - t0
-    return {"value": round(reps / dt, 4), "unit": "matvec/s", "cores": n, "kind": "port",
-            "sample": f"{reps} matvecs of the same 128x128x64 ComplexF64 self operator (numpy/scipy.fft "
+    return {"value": round(1 / dt, 4), "unit": "matvec/s", "cores": n, "kind": "port",
+            "sample": f"1 matvec of the same 256x256x128 ComplexF64 self operator (numpy/scipy.fft "
                       f"restatement of egoBrnHst!, FFT workers={n}, elementwise steps single-threaded)"}, x, y
 
 
 def oracle_check(gila, x, y_ref):
     """Relative L2 error of the GPU ComplexF64 and ComplexF32 matvecs of the
-    bench operator against the oracle's FP64 result on the same input (the
-    ComplexF32 operator holds the same kernel values rounded)."""
+    bench operator (256x256x128) against the oracle's FP64 result on the same
+    input (the ComplexF32 operator holds the same kernel values rounded)."""
     out = {}
     xf = np.asfortranarray(x)
     for dt, key in ((np.complex128, "rel_l2_f64"), (np.complex64, "rel_l2_f32")):
         mem, _ = make_opr(gila, CEL, dt)
         yg = np.asarray(gila.egoOpr(mem, xf.astype(dt))).astype(np.complex128)
         out[key] = float(np.linalg.norm((yg - y_ref).ravel()) / np.linalg.norm(y_ref.ravel()))
-        del mem
+        del mem, yg
     out["tolerance"] = {"f64": 1e-12, "f32": 1e-5}
-    out["input"] = "seeded N(0,1) current (seed 3) through the bench operator; oracle: FP64 restatement of egoBrnHst!"
+    out["input"] = ("seeded N(0,1) current (seed 3) through the 256x256x128 bench operator; oracle: FP64 "
+                    "restatement of egoBrnHst!")
     return out
 
 
@@ -753,36 +814,26 @@ def run_reference(a, world):
     """--impl reference: the reference's CPU path (egoBrnHst!, restated in
     the oracle; the Julia package cannot run on this image) on all host
     threads, same configuration and metric."""
-    from oracle.gla_mem import ExtInf, Vol
-    from oracle.matvec import OprMem, ego_opr, use_fft_workers
-    n = os.cpu_count() or 1
-    use_fft_workers(n)
-    v = Vol.make(CEL, SCL)
-    mix = ExtInf.make(v, v)
-    fur = synthetic_fur(tru_self(CEL), np.complex128, 1)
-    rng = np.random.default_rng(3)
-    x = rng.standard_normal((*CEL, 3)) + 1j * rng.standard_normal((*CEL, 3))
-    om = OprMem(mix, fur)
+    from oracle.matvec import ego_opr
+    om, x, n = _oracle_setup()
     t0 = time.perf_counter()
-    for _ in range(max(1, min(a.warmup, 2))):
-        ego_opr(om, x)
-    per = (time.perf_counter() - t0) / max(1, min(a.warmup, 2))
-    budget = 150.0
+    ego_opr(om, x)  # warm-up (one, to bound the CPU run)
+    per = time.perf_counter() - t0
+    budget = 60.0
     k = max(1, min(a.steps, int(budget / max(per, 1e-3))))
     t0 = time.perf_counter()
     for _ in range(k):
         ego_opr(om, x)
     dt = time.perf_counter() - t0
     val = k / dt
-    sample = (f"{k} of {a.steps} requested steps timed (1 matvec each; the rest skipped to bound the CPU run), "
-              f"numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n}")
-    out = {"impl": "reference", "metric": METRIC, "value": round(val, 4), "unit": "matvec/s", "n_gpus": world,
+    sample = (f"{k} of {a.steps} requested steps timed after 1 warm-up (1 matvec each; the rest skipped to bound "
+              f"the CPU run), numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n}")
+    out = {"impl": "reference", "metric": METRIC if a.dtype == "c128" else METRIC.replace("ComplexF64", "ComplexF32"),
+           "value": round(val, 4), "unit": "matvec/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / k * 1e3, 2), "higher_is_better": True,
            "scaling": "weak", "vs_baseline": None, "dtype": "f32" if a.dtype == "c64" else "f64",
-           "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel",
-           "config": {"workload": "self Green operator 128x128x64 cells, 1/32 wavelength, "
-                               + ("ComplexF32" if a.dtype == "c64" else "ComplexF64") + ", 1 vector/step",
-                      "parallelism": "host threads"},
+           "data": "synthetic: seeded N(0,1) currents, seeded synthetic Fourier kernel of the reference's storage shapes",
+           "config": bench_config(a.dtype == "c64", world),
            "cpu_baseline": {"value": round(val, 4), "unit": "matvec/s", "cores": n, "kind": "port", "sample": sample},
            "e2e": {"value": round(val, 4), "unit": "matvec/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(out), flush=True)

@@ -42,7 +42,7 @@ __all__ = [
     "GlaVol", "GlaKerOpt", "GlaOprMem", "GlaOpr", "egoOpr", "mul", "adjoint", "isadjoint",
     "isselfoperator", "isexternaloperator", "glaSze", "size", "eltype", "issymmetric",
     "isposdef", "ishermitian", "isdiag", "GilaError", "DimensionMismatch", "ArgumentError",
-    "Context", "default_context", "cast", "LippmannSchwinger", "solve", "SolveInfo", "SolveServer",
+    "Context", "default_context", "cast", "weak_integrals", "LippmannSchwinger", "solve", "SolveInfo", "SolveServer",
 ]
 
 
@@ -320,6 +320,33 @@ class GlaOprMem:
         _check(L.lib().gila_opr_export_fur(self._h, ptrs))
         return outs
 
+    def save(self, path: str):
+        """Write the operator's egoFur with its volumes and GlaKerOpt to a
+        GILAFUR1 file (the kernel cache the reference keeps with Serialization
+        / JLD2, test/runtests.jl:38-98, examples/GilaOperators.jl:28-55)."""
+        _check(L.lib().gila_opr_save(self._h, str(path).encode()))
+
+    @classmethod
+    def load(cls, path: str, setTyp=np.complex128, ctx: Optional[Context] = None) -> "GlaOprMem":
+        """The operator stored in a GILAFUR1 file, cast to setTyp."""
+        ctx = ctx or default_context()
+        h = ct.c_void_p()
+        _check(L.lib().gila_opr_load(ctx.handle, str(path).encode(), _dtype_code(setTyp), ct.byref(h)))
+        self = cls.__new__(cls)
+        self._h, self.ctx = h, ctx
+        self._fin_dims()
+        hdr = np.fromfile(str(path), dtype=np.uint8, count=768)
+        i32 = hdr[8:32].view("<i4")
+        frq = hdr[32:48].view("<f8")
+        vols = hdr[48:384].view("<i8").reshape(2, 7, 3)
+        mk = lambda v: GlaVol(v[0], [Fraction(int(n), int(d)) for n, d in zip(v[1], v[2])],  # noqa: E731
+                              [Fraction(int(n), int(d)) for n, d in zip(v[3], v[4])],
+                              [Fraction(int(n), int(d)) for n, d in zip(v[5], v[6])])
+        self.trgVol = mk(vols[0])
+        self.srcVol = self.trgVol if i32[2] else mk(vols[1])
+        self.cmpInf = GlaKerOpt(complex(frq[0], frq[1]), int(i32[4]), bool(i32[3]), True, (), ())
+        return self
+
     def reserve(self, nrhs: int):
         _check(L.lib().gila_opr_reserve(self._h, int(nrhs)))
 
@@ -406,6 +433,21 @@ class GlaOprMem:
             return torch.empty(s, dtype=like.dtype, device=like.device)
         s = (*shp[:3], 3, nrhs) if nrhs > 1 else (*shp[:3], 3)
         return np.empty(s, dtype=self.dtype, order="F")
+
+
+def weak_integrals(scl, frqPhz: complex = 1.0 + 0j, intOrd: int = 32, ctx: Optional[Context] = None):
+    """wekS, wekE, wekV (src/glaInt.jl:75-262) of a cell of size `scl` at
+    Gauss-Legendre order intOrd, evaluated on the GPU: (wS[3], wE[9], wV[6])
+    unscaled, as numpy complex arrays."""
+    ctx = ctx or default_context()
+    sr = [_rat(v) for v in scl]
+    num = (ct.c_int64 * 3)(*[r.numerator for r in sr])
+    den = (ct.c_int64 * 3)(*[r.denominator for r in sr])
+    out = (ct.c_double * 36)()
+    f = complex(frqPhz)
+    _check(L.lib().gila_weak_integrals(ctx.handle, num, den, f.real, f.imag, int(intOrd), out))
+    v = np.array(out[0::2]) + 1j * np.array(out[1::2])
+    return v[:3], v[3:12], v[12:18]
 
 
 def egoOpr(egoMem: GlaOprMem, actVec):

@@ -118,6 +118,11 @@ _SIGS = [
     ("gila_server_wait", ct.c_int, [ct.c_void_p, ct.c_uint64, ct.c_int64, ct.POINTER(GilaSolveInfoC),
                                     ct.POINTER(ct.c_double)]),
     ("gila_server_stats_get", ct.c_int, [ct.c_void_p, ct.POINTER(GilaServerStatsC)]),
+    ("gila_opr_save", ct.c_int, [ct.c_void_p, ct.c_char_p]),
+    ("gila_opr_load", ct.c_int, [ct.c_void_p, ct.c_char_p, ct.c_int, ct.POINTER(ct.c_void_p)]),
+    ("gila_weak_integrals", ct.c_int, [ct.c_void_p, ct.c_int64 * 3, ct.c_int64 * 3, ct.c_double, ct.c_double,
+                                       ct.c_int32, ct.c_double * 36]),
+    ("gila_debug_fail_alloc", ct.c_int, [ct.c_int64]),
     ("gila_opr_apply_noalloc", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p,
                                           ct.c_int64, ct.c_void_p]),
 ]

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <complex>
 #include <cstdio>
@@ -31,6 +32,23 @@ gila_status cuda_fail(cudaError_t e, const char* where) {
 }
 
 size_t csize(gila_dtype t) { return t == GILA_C128 ? 16 : 8; }
+
+// Fault injection for tests: when armed with n >= 1, the n-th device
+// allocation from then on fails as an out-of-memory would, before cudaMalloc
+// is called, and the countdown disarms.
+static std::atomic<int64_t> g_fail_alloc{0};
+
+cudaError_t dev_malloc_raw(void** p, size_t bytes) {
+  *p = nullptr;
+  int64_t n = g_fail_alloc.load();
+  while (n > 0) {
+    if (g_fail_alloc.compare_exchange_weak(n, n - 1)) {
+      if (n == 1) return cudaErrorMemoryAllocation;
+      break;
+    }
+  }
+  return cudaMalloc(p, bytes);
+}
 
 // ------------------------------------------------------------- rationals
 static int64_t gcd64(int64_t a, int64_t b) {
@@ -186,7 +204,7 @@ gila_status twiddle_table(Ctx* ctx, int P, gila_dtype dt, const void** out) {
   }
   void* d = nullptr;
   const size_t bytes = (size_t)P * csize(dt);
-  GILA_CUDA_TRY(cudaMalloc(&d, bytes));
+  GILA_CUDA_TRY(dev_malloc(&d, bytes));
   if (dt == GILA_C128) {
     std::vector<double2> h(P);
     for (int m = 0; m < P; ++m) h[m] = make_double2(re[m], im[m]);
@@ -345,10 +363,10 @@ gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* sr
     if ((s = plan_axis(g.P[k], &core->plan[k])) != GILA_OK) return s;
     if ((s = twiddle_table(ctx->impl, g.P[k], dtype, &core->tw[k])) != GILA_OK) return s;
     std::vector<int> m = axis_map(g.P[k], g.tru[k], g.tc[k]);
-    GILA_CUDA_TRY(cudaMalloc(&core->maps[k], m.size() * sizeof(int)));
+    GILA_CUDA_TRY(dev_malloc(&core->maps[k], m.size() * sizeof(int)));
     GILA_CUDA_TRY(cudaMemcpy(core->maps[k], m.data(), m.size() * sizeof(int), cudaMemcpyHostToDevice));
   }
-  GILA_CUDA_TRY(cudaMalloc(&core->plan_d, 3 * sizeof(AxisPlan)));
+  GILA_CUDA_TRY(dev_malloc(&core->plan_d, 3 * sizeof(AxisPlan)));
   GILA_CUDA_TRY(cudaMemcpy(core->plan_d, core->plan, 3 * sizeof(AxisPlan), cudaMemcpyHostToDevice));
   GILA_CUDA_TRY(cudaStreamCreateWithFlags(&core->stream, cudaStreamNonBlocking));
   return GILA_OK;
@@ -454,8 +472,8 @@ gila_status ensure_work(Core& c, int64_t nrhs) {
   cudaFree(c.B);
   c.A = c.B = nullptr;
   c.cap_rhs = 0;
-  GILA_CUDA_TRY(cudaMalloc(&c.A, (size_t)w.a_elems * cs));
-  GILA_CUDA_TRY(cudaMalloc(&c.B, (size_t)(w.b_rhs * nrhs) * cs));
+  GILA_CUDA_TRY(dev_malloc(&c.A, (size_t)w.a_elems * cs));
+  GILA_CUDA_TRY(dev_malloc(&c.B, (size_t)(w.b_rhs * nrhs) * cs));
   c.cap_rhs = nrhs;
   return GILA_OK;
 }
@@ -609,8 +627,8 @@ template <typename C>
 static gila_status tune_t(Core& c, int64_t nrhs, Launch& best, const Launch* keep_radix) {
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
   C *din = nullptr, *dout = nullptr;
-  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
-  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
+  GILA_CUDA_TRY(dev_malloc(&din, (size_t)ni * sizeof(C)));
+  cudaError_t e = dev_malloc(&dout, (size_t)no * sizeof(C));
   if (e == cudaSuccess) e = cudaMemsetAsync(din, 0, (size_t)ni * sizeof(C), c.stream);
   if (e != cudaSuccess) {
     cudaFree(din);
@@ -734,7 +752,7 @@ static gila_status ensure_stage(void*& buf, int64_t& cap, int64_t n, size_t cs) 
   cudaFree(buf);
   buf = nullptr;
   cap = 0;
-  GILA_CUDA_TRY(cudaMalloc(&buf, (size_t)n * cs));
+  GILA_CUDA_TRY(dev_malloc(&buf, (size_t)n * cs));
   cap = n;
   return GILA_OK;
 }
@@ -881,8 +899,8 @@ gila_status time_passes_t(Core& c, int64_t nrhs, int reps, double ms[4]) {
   if ((s = ensure_tuned(c, nrhs)) != GILA_OK) return s;
   const int64_t ni = in_elems(c) * nrhs, no = out_elems(c) * nrhs;
   C *din = nullptr, *dout = nullptr;
-  GILA_CUDA_TRY(cudaMalloc(&din, (size_t)ni * sizeof(C)));
-  cudaError_t e = cudaMalloc(&dout, (size_t)no * sizeof(C));
+  GILA_CUDA_TRY(dev_malloc(&din, (size_t)ni * sizeof(C)));
+  cudaError_t e = dev_malloc(&dout, (size_t)no * sizeof(C));
   if (e != cudaSuccess) {
     cudaFree(din);
     return cuda_fail(e, "cudaMalloc");
@@ -931,6 +949,12 @@ extern "C" {
 const char* gila_last_error(void) { return g_err.c_str(); }
 
 const char* gila_version(void) { return "0.1.0"; }
+
+gila_status gila_debug_fail_alloc(int64_t n) {
+  if (n < 0) return fail(GILA_ERR_ARG, "gila_debug_fail_alloc: n must be >= 0");
+  g_fail_alloc.store(n);
+  return GILA_OK;
+}
 
 const char* gila_status_string(gila_status s) {
   switch (s) {
@@ -995,7 +1019,7 @@ gila_status gila_opr_create_from_fur(gila_ctx* ctx, const gila_vol* trg, const g
         return fail(GILA_ERR_ARG, "egoFur branch " + std::to_string(eo) + " has extents that do not match the volumes");
   }
   const size_t bytes = (size_t)g.tru[0] * g.tru[1] * g.tru[2] * 6 * 8 * g.parT * csize(dtype);
-  GILA_CUDA_TRY(cudaMalloc(&core->ker, bytes));
+  GILA_CUDA_TRY(dev_malloc(&core->ker, bytes));
   core->ker_bytes = bytes;
   if (dtype == GILA_C128) {
     std::vector<double2> h;
@@ -1058,6 +1082,42 @@ gila_status gila_opr_export_fur(gila_opr* opr, void* const host_out[8]) {
   return GILA_OK;
 }
 
+// ---- kernel cache on disk ------------------------------------------------
+// File layout (little-endian), 768-byte header then the 8 egoFur arrays:
+//   0 "GILAFUR1" | 8 int32 version (1) | 12 int32 dtype of the arrays
+//   16 int32 self | 20 int32 adjMod | 24 int32 intOrd | 28 int32 0
+//   32 f64 frqPhz re | 40 f64 frqPhz im
+//   48 int64[21] target gila_vol | 216 int64[21] source gila_vol
+//   384 int64[8][6] branch extents (tx, ty, tz, 6, parSrc, parTrg)
+//   768 fur[0] ... fur[7], column-major complex (re, im) per element
+static const char kFurMagic[8] = {'G', 'I', 'L', 'A', 'F', 'U', 'R', '1'};
+constexpr size_t kFurHeader = 768;
+
+static void vol_pack(const gila_vol& v, int64_t out[21]) {
+  for (int k = 0; k < 3; ++k) {
+    out[k] = v.cel[k];
+    out[3 + k] = v.scl_num[k];
+    out[6 + k] = v.scl_den[k];
+    out[9 + k] = v.org_num[k];
+    out[12 + k] = v.org_den[k];
+    out[15 + k] = v.grd_num[k];
+    out[18 + k] = v.grd_den[k];
+  }
+}
+static gila_vol vol_unpack(const int64_t in[21]) {
+  gila_vol v;
+  for (int k = 0; k < 3; ++k) {
+    v.cel[k] = in[k];
+    v.scl_num[k] = in[3 + k];
+    v.scl_den[k] = in[6 + k];
+    v.org_num[k] = in[9 + k];
+    v.org_den[k] = in[12 + k];
+    v.grd_num[k] = in[15 + k];
+    v.grd_den[k] = in[18 + k];
+  }
+  return v;
+}
+
 gila_status gila_opr_adjoint(gila_opr* opr, gila_opr** out) {
   if (!opr || !out) return fail(GILA_ERR_ARG, "null argument");
   auto* o = new gila_opr;
@@ -1068,6 +1128,103 @@ gila_status gila_opr_adjoint(gila_opr* opr, gila_opr** out) {
   o->adj = !opr->adj;
   *out = o;
   return GILA_OK;
+}
+
+gila_status gila_opr_save(gila_opr* opr, const char* path) {
+  if (!opr || !opr->core || !path) return fail(GILA_ERR_ARG, "null argument");
+  const Core& c = *opr->core;
+  int64_t dims[8][6];
+  gila_status s = gila_opr_fur_dims(opr, dims);
+  if (s != GILA_OK) return s;
+  const size_t cs = csize(c.dtype);
+  std::vector<std::vector<unsigned char>> fur(8);
+  void* ptrs[8];
+  for (int eo = 0; eo < 8; ++eo) {
+    int64_t n = 1;
+    for (int k = 0; k < 6; ++k) n *= dims[eo][k];
+    fur[eo].resize((size_t)n * cs);
+    ptrs[eo] = fur[eo].data();
+  }
+  if ((s = gila_opr_export_fur(opr, ptrs)) != GILA_OK) return s;
+  unsigned char hdr[kFurHeader];
+  memset(hdr, 0, sizeof hdr);
+  memcpy(hdr, kFurMagic, 8);
+  const int32_t i32[6] = {1, (int32_t)c.dtype, c.self ? 1 : 0, (int32_t)(c.opt.adj_mod != 0),
+                          c.opt.int_ord > 0 ? c.opt.int_ord : 32, 0};
+  memcpy(hdr + 8, i32, sizeof i32);
+  const double frq[2] = {c.opt.frq_re, c.opt.frq_im};
+  memcpy(hdr + 32, frq, sizeof frq);
+  int64_t tv[21], sv[21];
+  vol_pack(vol_to_abi(c.trg), tv);
+  vol_pack(vol_to_abi(c.self ? c.trg : c.src), sv);
+  memcpy(hdr + 48, tv, sizeof tv);
+  memcpy(hdr + 216, sv, sizeof sv);
+  memcpy(hdr + 384, dims, sizeof dims);
+  FILE* f = fopen(path, "wb");
+  if (!f) return fail(GILA_ERR_ARG, std::string("cannot open ") + path + " for writing");
+  bool ok = fwrite(hdr, 1, sizeof hdr, f) == sizeof hdr;
+  for (int eo = 0; eo < 8 && ok; ++eo) ok = fwrite(fur[eo].data(), 1, fur[eo].size(), f) == fur[eo].size();
+  ok = (fclose(f) == 0) && ok;
+  if (!ok) return fail(GILA_ERR_INTERNAL, std::string("short write to ") + path);
+  return GILA_OK;
+}
+
+gila_status gila_opr_load(gila_ctx* ctx, const char* path, gila_dtype dtype, gila_opr** out) {
+  if (!ctx || !path || !out) return fail(GILA_ERR_ARG, "null argument");
+  if (dtype != GILA_C64 && dtype != GILA_C128) return fail(GILA_ERR_ARG, "unknown dtype");
+  FILE* f = fopen(path, "rb");
+  if (!f) return fail(GILA_ERR_ARG, std::string("cannot open ") + path);
+  unsigned char hdr[kFurHeader];
+  if (fread(hdr, 1, sizeof hdr, f) != sizeof hdr || memcmp(hdr, kFurMagic, 8) != 0) {
+    fclose(f);
+    return fail(GILA_ERR_ARG, std::string(path) + " is not a GILAFUR1 kernel file");
+  }
+  int32_t i32[6];
+  double frq[2];
+  int64_t tv[21], sv[21], dims[8][6];
+  memcpy(i32, hdr + 8, sizeof i32);
+  memcpy(frq, hdr + 32, sizeof frq);
+  memcpy(tv, hdr + 48, sizeof tv);
+  memcpy(sv, hdr + 216, sizeof sv);
+  memcpy(dims, hdr + 384, sizeof dims);
+  if (i32[0] != 1 || (i32[1] != GILA_C64 && i32[1] != GILA_C128)) {
+    fclose(f);
+    return fail(GILA_ERR_ARG, std::string(path) + ": unsupported GILAFUR version or dtype");
+  }
+  const gila_dtype fdt = (gila_dtype)i32[1];
+  const size_t cs = csize(fdt);
+  std::vector<std::vector<unsigned char>> fur(8);
+  const void* ptrs[8];
+  for (int eo = 0; eo < 8; ++eo) {
+    int64_t n = 1;
+    for (int k = 0; k < 6; ++k) {
+      if (dims[eo][k] < 1 || dims[eo][k] > (int64_t)1 << 20) {
+        fclose(f);
+        return fail(GILA_ERR_ARG, std::string(path) + ": corrupt branch extents");
+      }
+      n *= dims[eo][k];
+    }
+    if (n > ((int64_t)1 << 36) / (int64_t)cs) {
+      fclose(f);
+      return fail(GILA_ERR_ARG, std::string(path) + ": corrupt branch extents");
+    }
+    fur[eo].resize((size_t)n * cs);
+    if (fread(fur[eo].data(), 1, fur[eo].size(), f) != fur[eo].size()) {
+      fclose(f);
+      return fail(GILA_ERR_ARG, std::string(path) + ": file ends inside the kernel data");
+    }
+    ptrs[eo] = fur[eo].data();
+  }
+  fclose(f);
+  const gila_vol trg = vol_unpack(tv), src = vol_unpack(sv);
+  gila_kopt opt;
+  memset(&opt, 0, sizeof opt);
+  opt.frq_re = frq[0];
+  opt.frq_im = frq[1];
+  opt.int_ord = i32[4];
+  opt.adj_mod = i32[3];
+  opt.dev_mod = 1;
+  return gila_opr_create_from_fur(ctx, &trg, i32[2] ? nullptr : &src, &opt, dtype, ptrs, dims, fdt, out);
 }
 
 gila_status gila_opr_destroy(gila_opr* opr) {

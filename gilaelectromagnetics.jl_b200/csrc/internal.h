@@ -17,6 +17,15 @@ void set_error(const std::string& msg);
 gila_status fail(gila_status s, const std::string& msg);
 gila_status cuda_fail(cudaError_t e, const char* where);
 
+// Every device allocation of the library goes through dev_malloc, so that a
+// test can make the n-th one fail (gila_debug_fail_alloc) without touching
+// the GPU: the failure is returned before cudaMalloc is called.
+cudaError_t dev_malloc_raw(void** p, size_t bytes);
+template <typename T>
+inline cudaError_t dev_malloc(T** p, size_t bytes) {
+  return dev_malloc_raw(reinterpret_cast<void**>(p), bytes);
+}
+
 #define GILA_CUDA_TRY(expr)                                     \
   do {                                                          \
     cudaError_t e__ = (expr);                                   \

@@ -1327,14 +1327,15 @@ struct Build {
   gila_status alloc(T** out, size_t n) {
     DBuf* b = new DBuf;
     keep.push_back(b);
-    KB_TRY(cudaMalloc(&b->p, n * sizeof(T) + 16));
+    KB_TRY(dev_malloc(&b->p, n * sizeof(T) + 16));
     *out = static_cast<T*>(b->p);
     return GILA_OK;
   }
 };
 
-// weak values (18, scaled by 1/prod(scl)) for a cell of size scl
-static gila_status weak_values(Build& B, const Rat sclr[3], Z* w_d) {
+// weak values (18, scaled by 1/prod(scl)) for a cell of size scl; the
+// unscaled values go to raw_out when given
+static gila_status weak_values(Build& B, const Rat sclr[3], Z* w_d, Z* raw_out = nullptr) {
   const double scl[3] = {rd(sclr[0]), rd(sclr[1]), rd(sclr[2])};
   std::vector<WItem> items = weak_items(scl);
   const int n = (int)items.size(), ord = B.ord;
@@ -1347,7 +1348,10 @@ static gila_status weak_values(Build& B, const Rat sclr[3], Z* w_d) {
   int* nout_d;
   if ((s = B.alloc(&part_d, (size_t)n * max_outer)) != GILA_OK) return s;
   if ((s = B.alloc(&sums_d, n)) != GILA_OK) return s;
-  if ((s = B.alloc(&raw_d, 18)) != GILA_OK) return s;
+  if (raw_out)
+    raw_d = raw_out;
+  else if ((s = B.alloc(&raw_d, 18)) != GILA_OK)
+    return s;
   if ((s = B.alloc(&nout_d, n)) != GILA_OK) return s;
   std::vector<int> nout(n);
   for (int i = 0; i < n; ++i) {
@@ -1679,7 +1683,7 @@ gila_status build_kernel(Core& c) {
   const int parT = g.parT;
   const size_t cs = csize(c.dtype);
   const size_t per = (size_t)g.tru[0] * g.tru[1] * g.tru[2] * 6 * 8;  // elements per target partition
-  KB_TRY(cudaMalloc(&c.ker, per * parT * cs));
+  KB_TRY(dev_malloc(&c.ker, per * parT * cs));
   c.ker_bytes = per * parT * cs;
   const size_t mark = B.keep.size();
   for (int tp = 0; tp < parT; ++tp) {
@@ -1709,4 +1713,63 @@ gila_status build_kernel(Core& c) {
   return GILA_OK;
 }
 
+// wekS / wekE / wekV (src/glaInt.jl:75-262) for one cell scale at
+// Gauss-Legendre order `ord`, unscaled, evaluated on the GPU by the same
+// kernels the operator build uses (out: 18 complex values as re/im pairs,
+// wS[3], wE[9], wV[6]).
+gila_status weak_integrals(Ctx* ctx, const Rat scl[3], kb::Z f, int ord, double out[36]) {
+  using namespace kb;
+  if (ord < 1 || ord > kMaxOrd) return fail(GILA_ERR_ARG, "intOrd must be in 1..64");
+  for (int d = 0; d < 3; ++d)
+    if (scl[d].n <= 0 || scl[d].d <= 0) return fail(GILA_ERR_ARG, "cell scales must be positive");
+  cudaStream_t st = nullptr;
+  KB_TRY(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  gila_status s = GILA_OK;
+  {
+    Build B;
+    B.ctx = ctx;
+    B.st = st;
+    B.f = f;
+    B.ord = ord;
+    Consts q;
+    q.ord = ord;
+    gauss_legendre(ord, q.x, q.w);
+    q.f = f;
+    Z* w_d = nullptr;
+    Z raw[18];
+    if ((s = B.alloc(&B.q_d, 1)) == GILA_OK) {
+      cudaError_t e = cudaMemcpyAsync(B.q_d, &q, sizeof(q), cudaMemcpyHostToDevice, st);
+      if (e != cudaSuccess) s = cuda_fail(e, "cudaMemcpyAsync(weak consts)");
+    }
+    if (s == GILA_OK) s = B.alloc(&w_d, 36);
+    if (s == GILA_OK) s = weak_values(B, scl, w_d, w_d + 18);
+    if (s == GILA_OK) {
+      cudaError_t e = cudaMemcpyAsync(raw, w_d + 18, sizeof(raw), cudaMemcpyDeviceToHost, st);
+      if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+      if (e != cudaSuccess) s = cuda_fail(e, "weak integrals");
+    }
+    cudaStreamSynchronize(st);
+    if (s == GILA_OK)
+      for (int k = 0; k < 18; ++k) {
+        out[2 * k] = raw[k].x;
+        out[2 * k + 1] = raw[k].y;
+      }
+  }
+  cudaStreamDestroy(st);
+  return s;
+}
+
 }  // namespace gila
+
+extern "C" gila_status gila_weak_integrals(gila_ctx* ctx, const int64_t scl_num[3], const int64_t scl_den[3],
+                                           double frq_re, double frq_im, int32_t int_ord, double out[36]) {
+  using namespace gila;
+  if (!ctx || !scl_num || !scl_den || !out) return fail(GILA_ERR_ARG, "null argument");
+  GILA_CUDA_TRY(cudaSetDevice(ctx->impl->device));
+  Rat scl[3];
+  for (int d = 0; d < 3; ++d) {
+    if (scl_den[d] == 0) return fail(GILA_ERR_ARG, "zero denominator in a cell scale");
+    scl[d] = rat(scl_num[d], scl_den[d]);
+  }
+  return weak_integrals(ctx->impl, scl, kb::Z{frq_re, frq_im}, int_ord, out);
+}

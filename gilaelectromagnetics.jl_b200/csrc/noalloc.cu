@@ -2,12 +2,13 @@
 //
 // gila_opr_apply sizes its scratch workspaces (the x/y slab and the padded
 // spectrum between the passes) with cudaMalloc on first use.  Some callers
-// cannot let a library allocate at that point: code that records its work
-// into a CUDA stream capture (cudaMalloc is not a stream operation), hosts
-// whose own allocator owns every byte of device memory (a Julia or framework
-// memory pool), and latency-critical loops that forbid allocation after
-// start-up.  For them this entry point runs the same five passes with its
-// scratch in one fixed, file-scope device array instead.
+// cannot let a library allocate at that point: hosts whose own allocator owns
+// every byte of device memory (a Julia CUDA.jl or framework memory pool that
+// reserved the device at start-up, so a foreign cudaMalloc fails or steals
+// memory the pool has promised elsewhere), and latency-critical loops that
+// forbid allocation after start-up (cudaMalloc can synchronise the device and
+// takes an unbounded time).  For them this entry point runs the same five
+// passes with its scratch in one fixed, file-scope device array instead.
 //
 // The array is kNoAllocScratchBytes (64 MiB) and is reserved on every GPU that
 // loads the library, for the life of the process.  It is shared by every call
@@ -27,9 +28,11 @@ constexpr size_t kNoAllocScratchBytes = size_t(64) << 20;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-// Device address of g_noalloc_scratch, looked up once per device with that
-// device current.  (In host code the symbol names a host-side shadow, not a
-// device address, so it must never be handed to a kernel directly.)
+// Device address of g_noalloc_scratch, looked up once per device (the first
+// call on that device, with the device current) and kept for the process.
+// In host code the symbol names a host-side stand-in, not a device address,
+// so it is never handed to a kernel directly.  Like every operator's device
+// memory, the kept address does not survive cudaDeviceReset.
 static std::mutex g_na_mu;
 static void* g_na_ptr[128] = {};
 
@@ -71,15 +74,7 @@ static gila_status noalloc_t(Core& c, const void* in, void* out, cudaStream_t us
     return fail(GILA_ERR_INTERNAL, "no-alloc workspace plan exceeds the scratch");
   C* B = static_cast<C*>(scratch);
   C* A = reinterpret_cast<C*>(static_cast<unsigned char*>(scratch) + b_bytes);
-  DevOp<C> d;
-  d.ker = static_cast<const C*>(c.ker);
-  for (int k = 0; k < 3; ++k) {
-    d.map[k] = c.maps[k];
-    d.tw[k] = static_cast<const C*>(c.tw[k]);
-    d.plan[k] = c.plan[k];
-    d.plan_d[k] = c.plan_d + k;
-  }
-  d.scale = 1.0 / ((double)g.P[0] * g.P[1] * g.P[2]);
+  const DevOp<C> d = devop<C>(c);
   const Launch L = c.tuned ? c.launch : default_launch(c);
   cudaStream_t st = user_st ? user_st : c.stream;
   C one, zero;
@@ -118,6 +113,8 @@ extern "C" gila_status gila_opr_apply_noalloc(gila_opr* opr, gila_dtype dtype, c
     }
     if (a.type != cudaMemoryTypeDevice && a.type != cudaMemoryTypeManaged)
       return fail(GILA_ERR_ARG, "gila_opr_apply_noalloc takes device pointers only");
+    if (a.type == cudaMemoryTypeDevice && a.device != c.device)
+      return fail(GILA_ERR_ARG, "gila_opr_apply_noalloc: a vector lives on another GPU than the operator");
   }
   const size_t cs = csize(c.dtype);
   if ((uintptr_t)in % cs || (uintptr_t)out % cs)

@@ -521,6 +521,12 @@ gila_status gila_server_submit(gila_server* srv, const gila_vol* vol, const void
     rq.vol.grd_num[d] = r.n;
     rq.vol.grd_den[d] = r.d;
   }
+  {
+    const int64_t V = vol->cel[0] * vol->cel[1] * vol->cel[2];
+    gila_status s = check_finite(chi, V, "The medium (chi)");
+    if (s == GILA_OK) s = check_finite(b, 3 * V, "The incident field (b)");
+    if (s != GILA_OK) return s;
+  }
   rq.chi = chi;
   rq.b = b;
   rq.x = x;

@@ -551,7 +551,7 @@ struct DevArena {  // frees what it allocated when the solve returns
   }
   cudaError_t alloc(void** p, size_t bytes) {
     *p = nullptr;
-    cudaError_t e = cudaMalloc(p, bytes < 256 ? 256 : bytes);
+    cudaError_t e = dev_malloc(p, bytes < 256 ? 256 : bytes);
     if (e == cudaSuccess) d.push_back(*p);
     return e;
   }
@@ -1310,7 +1310,7 @@ gila_status cast_core(gila_ctx* ctx, Core& c, gila_dtype dtype, std::shared_ptr<
   if (s != GILA_OK) return s;
   const int64_t elems = (int64_t)(c.ker_bytes / csize(c.dtype));
   core->ker_bytes = (size_t)elems * csize(dtype);
-  GILA_CUDA_TRY(cudaMalloc(&core->ker, core->ker_bytes));
+  GILA_CUDA_TRY(dev_malloc(&core->ker, core->ker_bytes));
   const int blocks = (int)std::min<int64_t>((elems + 255) / 256, 148 * 16);
   if (dtype == GILA_C128)
     k_cast_any<double2><<<blocks, 256, 0, c.stream>>>(c.ker, c.dtype == GILA_C128, static_cast<double2*>(core->ker),
@@ -1320,6 +1320,50 @@ gila_status cast_core(gila_ctx* ctx, Core& c, gila_dtype dtype, std::shared_ptr<
                                                       elems);
   GILA_CUDA_TRY(cudaGetLastError());
   GILA_CUDA_TRY(cudaStreamSynchronize(c.stream));
+  return GILA_OK;
+}
+
+// NaN / Inf in a solve's inputs.  A non-finite medium or incident field
+// would otherwise surface only as breakdowns and restarts until the matvec
+// budget runs out; the reference's LippmannSchwinger has no check of its own,
+// the kernel build checks its output (src/glaMemSup.jl:93-95) and this check
+// extends that rule to the solve's inputs.
+__global__ void k_nonfinite(const double* __restrict__ p, int64_t n, int* __restrict__ flag) {
+  int bad = 0;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    bad |= !isfinite(p[i]);
+  if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(flag, 1);
+}
+
+gila_status check_finite(const void* p, int64_t n_complex, const char* what) {
+  const double* d = static_cast<const double*>(p);
+  const int64_t n = 2 * n_complex;
+  bool bad = false;
+  if (!is_device_ptr(p)) {
+    for (int64_t i = 0; i < n; ++i)
+      if (!std::isfinite(d[i])) {
+        bad = true;
+        break;
+      }
+  } else {
+    int* flag = nullptr;
+    GILA_CUDA_TRY(dev_malloc(&flag, sizeof(int)));
+    cudaStream_t st = nullptr;
+    cudaError_t e = cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking);
+    int h = 0;
+    if (e == cudaSuccess) e = cudaMemsetAsync(flag, 0, sizeof(int), st);
+    if (e == cudaSuccess) {
+      k_nonfinite<<<1184, 256, 0, st>>>(d, n, flag);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(&h, flag, sizeof(int), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (st) cudaStreamDestroy(st);
+    cudaFree(flag);
+    if (e != cudaSuccess) return cuda_fail(e, "finiteness check of solve inputs");
+    bad = h != 0;
+  }
+  if (bad) return fail(GILA_ERR_NAN, std::string(what) + " contains non-numeric values.");
   return GILA_OK;
 }
 
@@ -1375,6 +1419,8 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
     inner = g32->core.get();
   }
   GILA_CUDA_TRY(cudaSetDevice(a.device));
+  if ((s = check_finite(chi, in_elems(a) / 3, "The medium (chi)")) != GILA_OK) return s;
+  if ((s = check_finite(b, in_elems(a) * nrhs, "The incident field (b)")) != GILA_OK) return s;
   const bool keep = opts && opts->keep;
   char key[160];
   snprintf(key, sizeof key, "%p|%d|%d|%d|%d|%lld", (void*)inner, cfg.ell, cfg.mixed, cfg.graph, cfg.chi_shared,

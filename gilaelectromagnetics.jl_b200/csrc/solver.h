@@ -78,5 +78,8 @@ bool same_volume(const Core& a, const Core& b);
 // a copy of operator c in another precision (kernel cast on the device)
 gila_status cast_core(gila_ctx* ctx, Core& c, gila_dtype dtype, std::shared_ptr<Core>& out);
 gila_status check_ls_operator(const Core& a);
+// GILA_ERR_NAN when any of n_complex complex doubles at p (host or device
+// memory) is NaN or Inf; `what` names the input in the message
+gila_status check_finite(const void* p, int64_t n_complex, const char* what);
 
 }  // namespace gila

@@ -100,7 +100,7 @@ function GlaOprMem(cmpInf, trgVol, srcVol=nothing; egoFur=nothing, setTyp::DataT
             ctx(), tv, srcVol === nothing ? C_NULL : sv, o, code, r))
     else
         fur = [Array(f) for f in egoFur]                 # host copies, reference layout
-        ptrs = [pointer(f) for f in fur]
+        ptrs = Ptr{Cvoid}[pointer(f) for f in fur]
         dims = zeros(Int64, 6, 8)
         for e in 1:8, k in 1:6
             dims[k, e] = size(fur[e], k)
@@ -191,6 +191,83 @@ function LinearAlgebra.mul!(y::AbstractArray{T}, o::GlaOpr, x::AbstractArray{T},
         (Ptr{Cvoid}, Cint, Ptr{Cdouble}, Ptr{Cvoid}, Int64, Ptr{Cdouble}, Ptr{Cvoid}, Int64, Int64, Ptr{Cvoid}),
         o.mem.h, dtcode(T), a, pointer(x), length(x), b, pointer(y), length(y), 1, C_NULL))
     y
+end
+
+# ---- kernel cache files ----------------------------------------------------
+# The reference keeps egoFur between sessions with Serialization / JLD2
+# (test/runtests.jl:38-98, examples/GilaOperators.jl:28-55).  GILAFUR1 is the
+# library's raw little-endian format (layout in include/gila_b200.h,
+# gila_opr_save): a 768-byte header, then the 8 branches in the reference
+# layout.  readGilaFur / writeGilaFur read and write it in plain Julia, so a
+# kernel cached by either side feeds GlaOprMem(...; egoFur = fur) on the other.
+
+littleendian() = ENDIAN_BOM == 0x04030201 || error("GILAFUR files are little-endian; this host is not")
+
+function furvol(a::Vector{Int64})
+    scl = Tuple(a[4:6] .// a[7:9]); org = Tuple(a[10:12] .// a[13:15]); grd = Tuple(a[16:18] .// a[19:21])
+    (cel=Tuple(a[1:3]), scl=scl, org=org, grd=[StepRange(o, g, o) for (o, g) in zip(org, grd)])
+end
+
+"""Header of a GILAFUR1 file: element type, self flag, GlaKerOpt fields,
+volumes (after GlaOprMem's even-cell regeneration) and branch extents."""
+function readGilaFurHeader(io::IO)
+    littleendian()
+    String(read(io, 8)) == "GILAFUR1" || error("not a GILAFUR1 kernel file")
+    h = [read(io, Int32) for _ in 1:6]
+    h[1] == 1 || error("unsupported GILAFUR version $(h[1])")
+    frq = complex(read(io, Float64), read(io, Float64))
+    v = [read(io, Int64) for _ in 1:42]
+    dims = reshape([read(io, Int64) for _ in 1:48], 6, 8)
+    (T=h[2] == 1 ? ComplexF64 : ComplexF32, self=h[3] == 1, adjMod=h[4] == 1, intOrd=Int(h[5]),
+     frqPhz=frq, trgVol=furvol(v[1:21]), srcVol=furvol(v[22:42]), dims=dims)
+end
+readGilaFurHeader(path::AbstractString) = open(readGilaFurHeader, path, "r")
+
+"""(egoFur, header) of a GILAFUR1 file; egoFur is the Vector{Array{T,6}} that
+GlaOprMem(...; egoFur = egoFur) accepts (src/glaMemSup.jl:16-20)."""
+function readGilaFur(path::AbstractString)
+    open(path, "r") do io
+        meta = readGilaFurHeader(io)
+        seek(io, 768)
+        fur = [read!(io, Array{meta.T,6}(undef, Tuple(meta.dims[:, e])...)) for e in 1:8]
+        fur, meta
+    end
+end
+
+"""Write a reference egoFur (host or device arrays) with its operator's
+volumes and GlaKerOpt as a GILAFUR1 file that gila_opr_load reads."""
+function writeGilaFur(path::AbstractString, egoFur::AbstractVector, trgVol, srcVol, cmpInf)
+    littleendian()
+    T = eltype(egoFur[1])
+    slf = srcVol === nothing || srcVol == trgVol
+    open(path, "w") do io
+        write(io, b"GILAFUR1")
+        write(io, Int32(1), dtcode(T), Int32(slf), Int32(cmpInf.adjMod), Int32(cmpInf.intOrd), Int32(0))
+        write(io, Float64(real(cmpInf.frqPhz)), Float64(imag(cmpInf.frqPhz)))
+        for v in (trgVol, slf ? trgVol : srcVol)
+            c = cvol(v)
+            write(io, Int64[c.cel..., c.scl_num..., c.scl_den..., c.org_num..., c.org_den..., c.grd_num..., c.grd_den...])
+        end
+        write(io, Int64[size(egoFur[e], k) for k in 1:6, e in 1:8])
+        for e in 1:8
+            write(io, Array{T}(egoFur[e]))
+        end
+    end
+    nothing
+end
+
+"""Save an operator's kernel to a GILAFUR1 file (gila_opr_save)."""
+glaSave(m::GlaOprMem, path::AbstractString) =
+    check(ccall((:gila_opr_save, LIB), Cint, (Ptr{Cvoid}, Cstring), m.h, path))
+
+"""The operator stored in a GILAFUR1 file, cast to setTyp (gila_opr_load)."""
+function glaLoad(path::AbstractString; setTyp::DataType=ComplexF64)
+    r = Ref{Ptr{Cvoid}}(C_NULL)
+    check(ccall((:gila_opr_load, LIB), Cint, (Ptr{Cvoid}, Cstring, Cint, Ref{Ptr{Cvoid}}),
+                ctx(), path, dtcode(setTyp), r))
+    h = readGilaFurHeader(path)
+    opt = (frqPhz=h.frqPhz, intOrd=h.intOrd, adjMod=h.adjMod, numTrd=(), numBlk=())
+    GlaOprMem{setTyp}(r[], opt, h.trgVol, h.self ? h.trgVol : h.srcVol)
 end
 
 # ---- the scattering solve (examples/GilaOperators.jl:57-96) ---------------

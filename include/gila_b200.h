@@ -112,6 +112,37 @@ gila_status gila_opr_create_from_fur(gila_ctx* ctx, const gila_vol* trg, const g
 gila_status gila_opr_fur_dims(const gila_opr* opr, int64_t dims[8][6]);
 gila_status gila_opr_export_fur(gila_opr* opr, void* const host_out[8]);
 
+/* Kernel cache on disk.  The reference keeps egoFur between sessions with
+ * Serialization files in a Scratch space (test/runtests.jl:38-98) or JLD2
+ * files keyed by element type, cells and scale (examples/GilaOperators.jl:
+ * 28-55); both are Julia-only formats.  gila_opr_save writes the operator's
+ * egoFur (in the reference layout, the operator's dtype) with its volumes
+ * and GlaKerOpt to one little-endian file, "GILAFUR1":
+ *   0 "GILAFUR1" | 8 int32 version 1 | 12 int32 dtype (gila_dtype)
+ *   16 int32 self | 20 int32 adjMod | 24 int32 intOrd | 28 int32 0
+ *   32 double frqPhz re | 40 double frqPhz im
+ *   48 int64[21] target gila_vol | 216 int64[21] source gila_vol
+ *      (cel[3], scl_num[3], scl_den[3], org_num[3], org_den[3],
+ *       grd_num[3], grd_den[3])
+ *   384 int64[8][6] extents of fur[eo]: (tx, ty, tz, 6, parSrc, parTrg)
+ *   768 fur[0] .. fur[7]: column-major complex arrays, (re, im) interleaved.
+ * Volumes are stored after GlaOprMem's even-cell regeneration; an adjoint
+ * handle saves the operator it shares.  gila_opr_load reads such a file and
+ * creates the operator as gila_opr_create_from_fur would, casting the kernel
+ * to `dtype`.  julia/GilaB200.jl reads and writes the same format in plain
+ * Julia, so a cache moves between this library and the reference package. */
+gila_status gila_opr_save(gila_opr* opr, const char* path);
+gila_status gila_opr_load(gila_ctx* ctx, const char* path, gila_dtype dtype, gila_opr** out);
+
+/* wekS / wekE / wekV (src/glaInt.jl:75-262), the weakly singular self, edge
+ * and vertex face-pair integrals of a cell of size scl at Gauss-Legendre
+ * order int_ord, evaluated on the GPU by the kernels the operator build uses;
+ * the reference's quadrature-convergence check (test/intConTest.jl:6-35)
+ * calls them directly.  out: 18 complex values as (re, im) pairs, unscaled:
+ * wS[3], wE[9], wV[6]. */
+gila_status gila_weak_integrals(gila_ctx* ctx, const int64_t scl_num[3], const int64_t scl_den[3], double frq_re,
+                                double frq_im, int32_t int_ord, double out[36]);
+
 /* adjoint(opr) (src/glaLinAlg.jl:16-29): a new handle that shares the
  * operator's device memory, with adjMod flipped and the volumes swapped.  As
  * in the reference, the matvec itself ignores adjMod. */
@@ -290,19 +321,30 @@ gila_status gila_server_wait(gila_server* srv, uint64_t ticket, int64_t timeout_
                              double* latency_ms);
 gila_status gila_server_stats_get(gila_server* srv, gila_server_stats* out);
 
+/* Fault injection for tests (no counterpart in the reference): with n >= 1,
+ * the n-th device allocation the library makes from now on fails as an
+ * out-of-memory would (GILA_ERR_NOMEM), before cudaMalloc is called; n = 0
+ * disarms.  Process-wide. */
+gila_status gila_debug_fail_alloc(int64_t n);
+
 /* A matvec that allocates no device memory.  This entry point has no
  * counterpart in the reference.  It computes out = G * in for one vector,
  * like gila_opr_apply, for callers that cannot let the library call
- * cudaMalloc at apply time: code recording into a CUDA stream capture, hosts
- * whose own memory pool owns all device memory, loops that forbid allocation
- * after start-up.  The scratch between the passes lives in one fixed 64 MiB
- * device array that every GPU loading the library holds until the process
- * exits; operators whose padded spectrum does not fit are rejected with
- * GILA_ERR_SIZE.  `in` and `out` must be device pointers (host vectors would
- * need staging buffers).  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  All calls
- * on a device share the array and calls that overlap on the GPU race on it.
- * stream == NULL runs on the operator's stream and waits. */
+ * cudaMalloc at apply time: hosts whose own memory pool owns all device
+ * memory (a foreign cudaMalloc there fails or takes memory the pool has
+ * promised elsewhere), and loops that forbid allocation after start-up
+ * (cudaMalloc can synchronise the device and take unbounded time).  The
+ * scratch between the passes lives in one fixed 64 MiB device array that
+ * every GPU loading the library holds until the process exits; operators
+ * whose padded spectrum plus one x/y plane do not fit are rejected with
+ * GILA_ERR_SIZE.  `in` and `out` must be device pointers on the operator's
+ * GPU (host vectors would need staging buffers).  The first call on a device
+ * looks up the array's device address and keeps it; make that first call
+ * before any stream capture, and note that the kept address, like the
+ * operators' own device memory, does not survive cudaDeviceReset.  All calls
+ * on a device share the array, which keeps the last call's contents, and
+ * calls that overlap on the GPU race on it.  stream == NULL runs on the
+ * operator's stream and waits. */
 gila_status gila_opr_apply_noalloc(gila_opr* opr, gila_dtype dtype, const void* in, int64_t in_len,
                                    void* out, int64_t out_len, void* stream);
 

@@ -21,3 +21,8 @@ def test_reference_arm_json_line():
         assert k in line, k
     assert line["impl"] == "reference" and line["value"] > 0 and line["steps"] == 1
     assert line["e2e"]["h2d_bytes_per_step"] == 0 and line["cpu_baseline"]["kind"] == "port"
+    # the same workload and config dict as the GPU arm's line
+    sys.path.insert(0, ROOT)
+    import bench
+    assert line["config"] == bench.bench_config(False, 1)
+    assert line["metric"] == bench.METRIC
