@@ -1127,6 +1127,408 @@ __global__ void __launch_bounds__(zr_threads(TX, P), zr_min_blocks(zr_threads(TX
   }
 }
 
+// ------------------------------------------------------------------------
+// Fused z pass, FP64, for lines whose source and target each fill at most
+// half of the padded length (self operators and external ones whose z
+// extents do not exceed half of P).  Same transform as k_zf_ct with fewer
+// shared-memory round trips, FP64 instructions and barriers:
+//   * forward stage 0 (radix 8, span 1) reads the source z planes of B
+//     straight into registers, all of a thread's loads in flight at once,
+//     and runs radix-8 butterflies whose upper four inputs are the known
+//     zero padding;
+//   * the middle stages run the three components back to back with one set
+//     of twiddles per task and one barrier per component;
+//   * the fused stage (forward last stage, 3x3 multiply, inverse first
+//     stage) multiplies with FMA chains, flips the off-diagonal signs of the
+//     mirror rules with sign-bit XORs instead of FP64 multiplies, and keeps
+//     the next frequency's kernel values in flight;
+//   * the last inverse stage (radix 8) forms only the four outputs that fall
+//     in the target half and writes them straight to B.
+// Results agree with k_zf_ct to rounding (both are checked against the
+// oracle); every tile width and both task forms give identical bits.
+
+// radix-8 DFT of v[0..3] with v[4..7] == 0
+template <bool INV, typename C>
+__device__ __forceinline__ void bfly8_half_in(C* v) {
+  using T = typename Real<C>::T;
+  const T h = (T)0.70710678118654752440084436210484903928;
+  const C a = v[0], b = v[2], c = v[1], d = v[3];
+  const C ib = cmuli<INV>(b), id = cmuli<INV>(d);
+  C e[4] = {cadd(a, b), cadd(a, ib), csub(a, b), csub(a, ib)};
+  C o[4] = {cadd(c, d), cadd(c, id), csub(c, d), csub(c, id)};
+  const C o1 = o[1], o3 = o[3];
+  if (!INV) {
+    o[1] = cmake<C>(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    o[3] = cmake<C>(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+  } else {
+    o[1] = cmake<C>(h * (o1.x - o1.y), h * (o1.x + o1.y));
+    o[3] = cmake<C>(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+  }
+  o[2] = cmuli<INV>(o[2]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    v[k] = cadd(e[k], o[k]);
+    v[k + 4] = csub(e[k], o[k]);
+  }
+}
+
+// radix-8 DFT of v[0..7] whose outputs 0..3 only are needed (into v[0..3])
+template <bool INV, typename C>
+__device__ __forceinline__ void bfly8_half_out(C* v) {
+  using T = typename Real<C>::T;
+  const T h = (T)0.70710678118654752440084436210484903928;
+  C e[4] = {v[0], v[2], v[4], v[6]};
+  C o[4] = {v[1], v[3], v[5], v[7]};
+  Bfly<4, INV, C>::run(e, nullptr, 0);
+  Bfly<4, INV, C>::run(o, nullptr, 0);
+  const C o1 = o[1], o3 = o[3];
+  if (!INV) {
+    o[1] = cmake<C>(h * (o1.x + o1.y), h * (o1.y - o1.x));
+    o[3] = cmake<C>(h * (o3.y - o3.x), -h * (o3.x + o3.y));
+  } else {
+    o[1] = cmake<C>(h * (o1.x - o1.y), h * (o1.x + o1.y));
+    o[3] = cmake<C>(-h * (o3.x + o3.y), h * (o3.x - o3.y));
+  }
+  o[2] = cmuli<INV>(o[2]);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) v[k] = cadd(e[k], o[k]);
+}
+
+// a with both parts' signs flipped when f != 0: a sign-bit XOR on the high
+// words, no FP64 instruction
+__device__ __forceinline__ double2 cflip(double2 a, int f) {
+  const long long m = (long long)(f != 0) << 63;
+  return make_double2(__longlong_as_double(__double_as_longlong(a.x) ^ m),
+                      __longlong_as_double(__double_as_longlong(a.y) ^ m));
+}
+
+// s * (g0 a + g1 b + g2 c) as two FMA chains
+__device__ __forceinline__ double2 mac3(const double2& g0, const double2& a, const double2& g1, const double2& b,
+                                       const double2& g2, const double2& c, double s) {
+  double re = g0.x * a.x;
+  re = fma(-g0.y, a.y, re);
+  re = fma(g1.x, b.x, re);
+  re = fma(-g1.y, b.y, re);
+  re = fma(g2.x, c.x, re);
+  re = fma(-g2.y, c.y, re);
+  double im = g0.x * a.y;
+  im = fma(g0.y, a.x, im);
+  im = fma(g1.x, b.y, im);
+  im = fma(g1.y, b.x, im);
+  im = fma(g2.x, c.y, im);
+  im = fma(g2.y, c.x, im);
+  return make_double2(re * s, im * s);
+}
+
+// the 3x3 symmetric multiply of one frequency (stored kernel g: xx, yy, zz,
+// xy, xz, yz; mirror flags rx, ry, rz), scaled by s
+__device__ __forceinline__ void zmul3f(double2& x0, double2& x1, double2& x2, const double2 (&g)[6], int rx, int ry,
+                                       int rz, double s) {
+  const double2 gxy = cflip(g[3], rx ^ ry), gxz = cflip(g[4], rx ^ rz), gyz = cflip(g[5], ry ^ rz);
+  const double2 a = x0, b = x1, c = x2;
+  x0 = mac3(g[0], a, gxy, b, gxz, c, s);
+  x1 = mac3(gxy, a, g[1], b, gyz, c, s);
+  x2 = mac3(gxz, a, gyz, b, g[2], c, s);
+}
+
+template <int P>
+constexpr bool zg_ok() {
+  return ct_nst(P) >= 3 && ct_radix(P, 0) == 8 && ct_radix(P, ct_nst(P) - 1) <= 4;
+}
+
+// One in-place middle stage S (radix order REV) over the three component
+// blocks of the tile, twiddles computed once per task.  Input index q of a
+// line sits in slot slot(q); outputs go to their natural slots.  One barrier
+// per component, between its loads and its stores; the stores of one stage
+// and the loads of the next are ordered by the barriers of the components
+// in between (callers put a barrier before a stage that follows a stage
+// writing all three components at once).
+template <int P, int S, int T, int TX, bool INV, bool REV, class Slot>
+__device__ __forceinline__ void zg_mid(double2* sm, const double2* __restrict__ tw, const Slot& slot) {
+  constexpr int R = ct_radix_o<REV>(P, S), NS = ct_span_o<REV>(P, S), TPL = P / R, NT = TX * TPL;
+  constexpr int K = (NT + T - 1) / T, TWST = P / (NS * R), CH = P * TX;
+  double2 w[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    const int j = task / TX;
+    if (NS > 1) twiddles<R, INV>(tw, (j % NS) * TWST, w[k]);
+  }
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    double2* const smc = sm + c * CH;
+    double2 v[K][R];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NT % T == 0 || task < NT) {
+        const int l = task % TX, j = task / TX;
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[k][r] = smc[slot(j + r * TPL) * TX + l];
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NT % T == 0 || task < NT) {
+        const int l = task % TX, j = task / TX, jm = j % NS;
+        if (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) v[k][r] = cmul(v[k][r], w[k][r]);
+        }
+        Bfly<R, INV, double2>::run(v[k], tw, TPL);
+        const int base = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r) smc[(base + r * NS) * TX + l] = v[k][r];
+      }
+    }
+  }
+}
+
+template <int P, int TX>
+__global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX, P))) k_zg_ct(const ZParams<double2> p) {
+  using C = double2;
+  constexpr int T = ct_threads(TX, P);
+  constexpr int CH = P * TX;
+  constexpr int NST = ct_nst(P);
+  constexpr int RL = ct_radix(P, NST - 1);  // last forward radix = first inverse radix
+  constexpr int TPL = P / RL;
+  constexpr int TPL0 = P / 8, NT0 = TX * TPL0, K0 = (NT0 + T - 1) / T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nrhs = p.nrhs, ntiles = p.ntiles, Px = p.Px, Py = p.Py;
+  const int nin = p.nin, nout = p.nout;
+  const int rhs = blockIdx.x % nrhs;
+  const int rest = blockIdx.x / nrhs;
+  const int tseq = rest % ntiles;
+  const int yseq = rest / ntiles;
+  const int kx0 = tile_seq(tseq, ntiles) * TX;
+  const int ky = mirror_seq(yseq, Py);
+  const int tmax = Px - kx0;
+  const int64_t plane = (int64_t)Py * Px;
+  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
+  const C* const tw = p.tw;
+  // forward stage 0: task (l, j0) reads z = j0 + r * TPL0, r < 4 (the upper
+  // half of the padded line is zero); output slot j0 * 8 + r
+  {
+    C v[3][K0][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        const int l = task % TX, j0 = task / TX;
+        const bool ok = (NT0 % T == 0 || task < NT0) && l < tmax;
+        const C* const src = Bb + (int64_t)c * nin * plane + l;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = j0 + r * TPL0;
+          v[c][k][r] = (ok && i < nin) ? __ldcs(src + (int64_t)i * plane) : czero<C>();
+        }
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        if (NT0 % T == 0 || task < NT0) {
+          const int l = task % TX, j0 = task / TX;
+          bfly8_half_in<false>(v[c][k]);
+          C* const dst = sm + c * CH + (j0 * 8) * TX + l;
+#pragma unroll
+          for (int r = 0; r < 8; ++r) dst[r * TX] = v[c][k][r];
+        }
+      }
+  }
+  __syncthreads();
+  // forward middle stages 1 .. NST-2
+  {
+    auto nat = [](int q) { return q; };
+    if constexpr (NST >= 3) zg_mid<P, 1, T, TX, false, false>(sm, tw, nat);
+    if constexpr (NST >= 4) zg_mid<P, 2, T, TX, false, false>(sm, tw, nat);
+    if constexpr (NST >= 5) zg_mid<P, 3, T, TX, false, false>(sm, tw, nat);
+  }
+  int py, iy, ry;
+  ax_map(p.ax[1], ky, py, iy, ry);
+  const int tx = p.tx, ty = p.ty, tz = p.tz;
+  const double s = p.scale;
+  auto kload = [&](int px, int ix, int f, C (&g)[6], int& rz) {
+    int pz, iz;
+    ax_map(p.ax[2], f, pz, iz, rz);
+    const C* gp = ker_at(p.ker, 4 * px + 2 * py + pz, iz, iy, ix, tx, ty, tz);
+#pragma unroll
+    for (int q = 0; q < 6; ++q) g[q] = ker_ld(gp, q, tx);
+  };
+  bool paired = false;
+  if constexpr (zm_ok<C, P>()) {
+    if (p.zmir && !p.ax[2].full) {
+      // mirror pairs of z frequencies (see k_zf_ct): frequency j + r*TPL of
+      // task j and P - j - r*TPL of task TPL - j read the same stored entry
+      constexpr int NPT = TX * (TPL / 2);
+      constexpr int K2 = (NPT + T - 1) / T;
+#pragma unroll
+      for (int k = 0; k < K2; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        const bool live = (NPT % T == 0 || task < NPT) && task % TX < tmax;
+        const int l = task % TX, jp = task / TX;
+        const int jj[2] = {jp, jp ? TPL - jp : TPL / 2};
+        int px = 0, ix = 0, rx = 0;
+        ax_map(p.ax[0], kx0 + l, px, ix, rx);
+        // the first frequency's kernel values go out before the barrier
+        C g[6];
+        int rzg = 0;
+        if (live) kload(px, ix, jj[0], g, rzg);
+        if (k == 0) __syncthreads();
+        if (!live) continue;
+        C v[2][3][RL];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+#pragma unroll
+          for (int c = 0; c < 3; ++c)
+#pragma unroll
+            for (int r = 0; r < RL; ++r) v[h][c][r] = sm[c * CH + (jj[h] + r * TPL) * TX + l];
+          C w[RL];
+          twiddles<RL, false>(tw, jj[h], w);
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+#pragma unroll
+            for (int r = 1; r < RL; ++r) v[h][c][r] = cmul(v[h][c][r], w[r]);
+            Bfly<RL, false, C>::run(v[h][c], tw, TPL);
+          }
+        }
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const int f0 = jj[0] + r * TPL, f1 = jj[1] + (RL - 1 - r) * TPL;
+          int pz0, iz0, rz0, pz1, iz1, rz1;
+          ax_map(p.ax[2], f0, pz0, iz0, rz0);
+          ax_map(p.ax[2], f1, pz1, iz1, rz1);
+          zmul3f(v[0][0][r], v[0][1][r], v[0][2][r], g, rx, ry, rz0, s);
+          if (pz1 != pz0 || iz1 != iz0) {
+            // the self-mirrored pair (0, TPL/2): its own entry
+            C g1[6];
+            int rzx = 0;
+            kload(px, ix, f1, g1, rzx);
+            zmul3f(v[1][0][RL - 1 - r], v[1][1][RL - 1 - r], v[1][2][RL - 1 - r], g1, rx, ry, rz1, s);
+          } else {
+            zmul3f(v[1][0][RL - 1 - r], v[1][1][RL - 1 - r], v[1][2][RL - 1 - r], g, rx, ry, rz1, s);
+          }
+          // next frequency's entry (two tasks' values already fill the
+          // registers: no second set in flight)
+          if (r + 1 < RL) kload(px, ix, jj[0] + (r + 1) * TPL, g, rzg);
+        }
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+          for (int c = 0; c < 3; ++c) {
+            Bfly<RL, true, C>::run(v[h][c], tw, TPL);
+#pragma unroll
+            for (int r = 0; r < RL; ++r) sm[c * CH + (jj[h] + r * TPL) * TX + l] = v[h][c][r];
+          }
+      }
+      paired = true;
+    }
+  }
+  if (!paired) {
+    constexpr int NTASK = TX * TPL;
+    constexpr int K = (NTASK + T - 1) / T;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      const bool live = (NTASK % T == 0 || task < NTASK) && task % TX < tmax;
+      const int l = task % TX, j = task / TX;
+      int px = 0, ix = 0, rx = 0;
+      ax_map(p.ax[0], kx0 + l, px, ix, rx);
+      // the first frequency's kernel values go out before the barrier
+      C g[6];
+      int rz = 0;
+      if (live) kload(px, ix, j, g, rz);
+      if (k == 0) __syncthreads();
+      if (!live) continue;
+      C v[3][RL];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) v[c][r] = sm[c * CH + (j + r * TPL) * TX + l];
+      {
+        C w[RL];
+        twiddles<RL, false>(tw, j, w);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int r = 1; r < RL; ++r) v[c][r] = cmul(v[c][r], w[r]);
+          Bfly<RL, false, C>::run(v[c], tw, TPL);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        C gn[6];
+        int rzn = 0;
+        if (r + 1 < RL) kload(px, ix, j + (r + 1) * TPL, gn, rzn);
+        zmul3f(v[0][r], v[1][r], v[2][r], g, rx, ry, rz, s);
+        if (r + 1 < RL) {
+#pragma unroll
+          for (int q = 0; q < 6; ++q) g[q] = gn[q];
+          rz = rzn;
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Bfly<RL, true, C>::run(v[c], tw, TPL);
+#pragma unroll
+        for (int r = 0; r < RL; ++r) sm[c * CH + (j + r * TPL) * TX + l] = v[c][r];
+      }
+    }
+  }
+  __syncthreads();
+  // inverse middle stages 1 .. NST-2 (reversed radix order); stage 1 reads
+  // through the fused stage's permutation (input q in slot q/RL + (q%RL)*TPL)
+  {
+    auto perm = [](int q) { return (q / RL) + (q % RL) * TPL; };
+    auto nat = [](int q) { return q; };
+    if constexpr (NST >= 3) zg_mid<P, 1, T, TX, true, true>(sm, tw, perm);
+    if constexpr (NST >= 4) zg_mid<P, 2, T, TX, true, true>(sm, tw, nat);
+    if constexpr (NST >= 5) zg_mid<P, 3, T, TX, true, true>(sm, tw, nat);
+  }
+  __syncthreads();
+  // inverse last stage (radix 8, span TPL0): outputs z = j + r * TPL0, r < 4
+  // (the target half), straight to the target z planes of B
+  {
+    constexpr int NSL = TPL0;
+    double2 w[K0][8];
+#pragma unroll
+    for (int k = 0; k < K0; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      twiddles<8, true>(tw, task / TX, w[k]);
+    }
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      const C* const smc = sm + c * CH;
+      C* const Bo = Bb + (int64_t)c * nout * plane;
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        if (NT0 % T == 0 || task < NT0) {
+          const int l = task % TX, j = task / TX;
+          C v[8];
+#pragma unroll
+          for (int r = 0; r < 8; ++r) v[r] = smc[(j + r * NSL) * TX + l];
+#pragma unroll
+          for (int r = 1; r < 8; ++r) v[r] = cmul(v[r], w[k][r]);
+          bfly8_half_out<true>(v);
+          if (l < tmax) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int i = j + r * NSL;
+              if (i < nout) Bo[(int64_t)i * plane + l] = v[r];
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 // The fused z pass for FP32 on line pairs (ct_stage2): same arithmetic as
 // k_zf_ct, each task moving two adjacent kx lines per shared-memory access.
 #ifndef GILA_ZF2_CAP
@@ -1351,6 +1753,15 @@ static bool ct_has(int P) {
 static inline bool zfuse() {
   static const bool on = [] {
     const char* e = getenv("GILA_ZFUSE");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
+// FP64 fused z pass with register-fed first stage and pruned half
+// butterflies (k_zg_ct) where it applies (GILA_ZG=0: k_zf_ct)
+static inline bool zgo() {
+  static const bool on = [] {
+    const char* e = getenv("GILA_ZG");
     return !(e && e[0] == '0');
   }();
   return on;
@@ -1621,6 +2032,12 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
           cudaError_t er = set_smem(fnr, sm);         \
           if (er != cudaSuccess) return er;           \
           k_zr_ct<C, n, tx><<<(unsigned)blocks, zr_threads(tx, n), sm, st>>>(p); \
+          return cudaGetLastError();                  \
+        }                                             \
+      }                                               \
+      if constexpr (sizeof(C) == 16 && zg_ok<n>()) {  \
+        if (p.parT == 1 && zfuse() && zgo() && 2 * p.nin <= n && 2 * p.nout <= n) { \
+          GILA_LAUNCH(false, (k_zg_ct<n, tx>), p);    \
           return cudaGetLastError();                  \
         }                                             \
       }                                               \
