@@ -576,21 +576,29 @@ static gila_status tune_on(Core& c, const Geom& g, int64_t nrhs, const C* din, C
     best.z_tx = pick;
     best.z_mir = pick_mir;
   }
-  if (yc.size() > 1 && e == cudaSuccess) {
+  // y tile width jointly with the form of the x / y passes (first stage fed
+  // from global memory, or staged through shared memory: the same
+  // arithmetic, the faster one depends on length and precision)
+  if (!yc.empty() && e == cudaSuccess) {
     float bt = 1e30f;
-    int pick = best.y_tx;
-    for (int tx : yc) {
-      Launch L = best;
-      L.y_tx = tx;
-      const float t = time_of(L, {0, 2});
-      if (e != cudaSuccess) break;
-      if (tune_debug()) fprintf(stderr, "gila autotune dtype %d y tile %d: %.4f ms\n", (int)c.dtype, tx, t);
-      if (t < bt) {
-        bt = t;
-        pick = tx;
+    int pick = best.y_tx, pick_g = best.xy_g;
+    for (int tx : yc)
+      for (int gf = 0; gf < 2 && e == cudaSuccess; ++gf) {
+        Launch L = best;
+        L.y_tx = tx;
+        L.xy_g = gf;
+        const float t = time_of(L, {0, 2});
+        if (e != cudaSuccess) break;
+        if (tune_debug())
+          fprintf(stderr, "gila autotune dtype %d y tile %d global-fed x/y %d: %.4f ms\n", (int)c.dtype, tx, gf, t);
+        if (t < bt) {
+          bt = t;
+          pick = tx;
+          pick_g = gf;
+        }
       }
-    }
     best.y_tx = pick;
+    best.xy_g = pick_g;
   }
   // radix order of the x and y passes: the greedy one (radix-8 stages first)
   // or its reverse, where they differ (specialised lengths, radix list not a

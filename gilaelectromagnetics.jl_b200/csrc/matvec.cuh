@@ -74,6 +74,9 @@ struct Launch {
   int x_rev = 0;  // radix order of the x passes: 0 greedy (8s first), 1 reversed
   int y_rev = 0;  // radix order of the y passes
   int z_mir = 1;  // fused z pass: one task per mirror pair of z frequencies
+  int xy_g = 1;   // x / y passes: first stage fed from global memory and half
+                  // last stage (1) or the line staged in shared memory (0);
+                  // the same arithmetic either way
 };
 
 // Lippmann-Schwinger epilogue of the last pass (self operators): out =

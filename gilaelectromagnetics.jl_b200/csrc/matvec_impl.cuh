@@ -1520,12 +1520,445 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
 #pragma unroll
             for (int r = 0; r < 4; ++r) {
               const int i = j + r * NSL;
-              if (i < nout) Bo[(int64_t)i * plane + l] = v[r];
+              if (i < nout) __stcs(Bo + (int64_t)i * plane + l, v[r]);
             }
           }
         }
       }
     }
+  }
+}
+
+// ------------------------------------------------------------------------
+// x and y passes (FP64) whose first stage is fed from global memory and
+// whose last stage forms only the target half: the forward passes load only
+// the source half of each padded line (radix-R0 butterflies with the upper
+// inputs known zero), every thread's loads in flight at once, instead of
+// staging the line through shared memory; the inverse passes load the full
+// spectrum line the same way and run a last butterfly that forms only the
+// outputs inside the target.  One shared-memory round trip per element
+// fewer than k_xfwd_ct / k_y_ct / k_xinv_ct, and fewer FP64 operations.
+
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void bfly_half_in(C* v) {
+  if constexpr (R == 8) {
+    bfly8_half_in<INV>(v);
+  } else if constexpr (R == 4) {
+    const C a = v[0], b = v[1], ib = cmuli<INV>(v[1]);
+    v[0] = cadd(a, b);
+    v[1] = cadd(a, ib);
+    v[2] = csub(a, b);
+    v[3] = csub(a, ib);
+  } else {
+    static_assert(R == 2, "half-input butterflies: radix 2, 4, 8");
+    v[1] = v[0];
+  }
+}
+
+template <int R, bool INV, typename C>
+__device__ __forceinline__ void bfly_half_out(C* v) {
+  if constexpr (R == 8) {
+    bfly8_half_out<INV>(v);
+  } else if constexpr (R == 4) {
+    const C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    const C t2 = cadd(v[1], v[3]), t3 = cmuli<INV>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[1] = cadd(t1, t3);
+  } else {
+    static_assert(R == 2, "half-output butterflies: radix 2, 4, 8");
+    v[0] = cadd(v[0], v[1]);
+  }
+}
+
+constexpr bool pow2_radix(int r) { return r == 2 || r == 4 || r == 8; }
+template <int P, bool REV>
+constexpr bool xyg_in_ok() {
+  return ct_nst(P) >= 2 && pow2_radix(ct_radix_o<REV>(P, 0));
+}
+template <int P, bool REV>
+constexpr bool xyg_out_ok() {
+  return ct_nst(P) >= 2 && pow2_radix(ct_radix_o<REV>(P, ct_nst(P) - 1));
+}
+
+// Stage 0 (span 1) fed from global memory: task (l, j) loads inputs j + r *
+// (P / R0) with gld(l, i), r < R0 / 2 when HALF (the rest is the zero
+// padding), then butterflies and st(l, j * R0 + r, v).
+template <typename C, int P, int T, int M, bool INV, bool LINE_FAST, bool REV, bool HALF, class GLd, class St>
+__device__ __forceinline__ void ct_first_g(const GLd& gld, const St& st) {
+  constexpr int R = ct_radix_o<REV>(P, 0), TPL = P / R, NT = M * TPL, K = (NT + T - 1) / T;
+  constexpr int RIN = HALF ? R / 2 : R;
+  C v[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int l = LINE_FAST ? task % M : task / TPL, j = LINE_FAST ? task / M : task % TPL;
+#pragma unroll
+      for (int r = 0; r < RIN; ++r) v[k][r] = gld(l, j + r * TPL);
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int l = LINE_FAST ? task % M : task / TPL, j = LINE_FAST ? task / M : task % TPL;
+      if constexpr (HALF)
+        bfly_half_in<R, INV>(v[k]);
+      else
+        Bfly<R, INV, C>::run(v[k], nullptr, TPL);
+#pragma unroll
+      for (int r = 0; r < R; ++r) st(l, j * R + r, v[k][r]);
+    }
+  }
+}
+
+// Last stage (span P / R) forming outputs j + r * (P / R) for r < R / 2
+// only: ld reads the stage input, st takes the outputs.
+template <typename C, int P, int T, int M, bool INV, bool LINE_FAST, bool REV, class Ld, class St>
+__device__ __forceinline__ void ct_last_half(const C* __restrict__ tw, const Ld& ld, const St& st) {
+  constexpr int S = ct_nst(P) - 1;
+  constexpr int R = ct_radix_o<REV>(P, S), NS = ct_span_o<REV>(P, S), TPL = P / R, NT = M * TPL;
+  constexpr int K = (NT + T - 1) / T, TWST = P / (NS * R);
+  static_assert(NS == TPL, "the last stage spans P / R");
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int l = LINE_FAST ? task % M : task / TPL, j = LINE_FAST ? task / M : task % TPL;
+      C v[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[r] = ld(l, j + r * TPL);
+      C w[R];
+      twiddles<R, INV>(tw, j * TWST, w);
+#pragma unroll
+      for (int r = 1; r < R; ++r) v[r] = cmul(v[r], w[r]);
+      bfly_half_out<R, INV>(v);
+#pragma unroll
+      for (int r = 0; r < R / 2; ++r) st(l, j + r * NS, v[r]);
+    }
+  }
+}
+
+template <int P, bool REV>
+__global__ void __launch_bounds__(ct_threads(ct_xlines<16>(P), P)) k_xfwd_g(const XfParams<double2> p) {
+  using C = double2;
+  constexpr int M = ct_xlines<16>(P);
+  constexpr int T = ct_threads(M, P);
+  constexpr int LS = P + (P + 7) / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nin = p.nin;
+  const int64_t rows = p.rows;
+  C* const A = p.A;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const C* const src = p.in + g0 * nin;
+  auto gld = [=](int l, int i) -> C {
+    return (g0 + l < rows && i < nin) ? __ldcs(src + (int64_t)l * nin + i) : czero<C>();
+  };
+  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
+  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int l, int i, C v) {
+    const int64_t g = g0 + l;
+    if (g < rows) A[g * P + i] = v;
+  };
+  ct_first_g<C, P, T, M, false, false, REV, true>(gld, sts);
+  __syncthreads();
+  ct_run_range<C, P, 1, 1, ct_nst(P), 8, T, M, false, false, REV>(p.tw, lds, lds, sts, stg, true, false);
+}
+
+template <int P, bool INV, int TX, bool REV>
+__global__ void __launch_bounds__(ct_threads(TX, P), pow2_min_blocks(ct_threads(TX, P), P)) k_y_g(const YParams<double2> p) {
+  using C = double2;
+  constexpr int T = ct_threads(TX, P);
+  constexpr int NST = ct_nst(P);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int Px = p.Px, nin = p.nin, nout = p.nout;
+  const int tile = blockIdx.x % p.ntiles;
+  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int64_t rc = slice / p.nz;
+  const int z = (int)(slice % p.nz);
+  const int kx0 = tile * TX;
+  const C* const src = p.src + ((rc * p.src_z + z) - p.src_sub) * p.src_rows * (int64_t)Px + kx0;
+  C* const dst = p.dst + ((rc * p.dst_z + z) - p.dst_sub) * p.dst_rows * (int64_t)Px + kx0;
+  const int tmax = Px - kx0;
+  auto gld = [=](int t, int i) -> C {
+    return (t < tmax && i < nin) ? __ldcs(src + (int64_t)i * Px + t) : czero<C>();
+  };
+  auto lds = [=](int t, int i) -> C { return sm[i * TX + t]; };
+  auto sts = [=](int t, int i, C v) { sm[i * TX + t] = v; };
+  auto stg = [=](int t, int i, C v) {
+    if (t < tmax && i < nout) {
+      // the forward pass writes the spectrum B (streamed through L2), the
+      // inverse pass the x/y slab that the x-inverse pass reads next
+      if constexpr (!INV)
+        __stcs(dst + (int64_t)i * Px + t, v);
+      else
+        dst[(int64_t)i * Px + t] = v;
+    }
+  };
+  if constexpr (!INV) {
+    ct_first_g<C, P, T, TX, false, true, REV, true>(gld, sts);
+    __syncthreads();
+    ct_run_range<C, P, 1, 1, NST, 8, T, TX, false, true, REV>(p.tw, lds, lds, sts, stg, true, false);
+  } else {
+    ct_first_g<C, P, T, TX, true, true, REV, false>(gld, sts);
+    __syncthreads();
+    ct_run_range<C, P, 1, 1, NST - 1, 8, T, TX, true, true, REV>(p.tw, lds, lds, sts, sts, true, true);
+    ct_last_half<C, P, T, TX, true, true, REV>(p.tw, lds, stg);
+  }
+}
+
+template <int P, bool AXPBY, bool REV>
+__global__ void __launch_bounds__(ct_threads(ct_xlines<16>(P), P)) k_xinv_g(const XiParams<double2> p) {
+  using C = double2;
+  constexpr int M = ct_xlines<16>(P);
+  constexpr int T = ct_threads(M, P);
+  constexpr int LS = P + (P + 7) / 8;
+  constexpr int NST = ct_nst(P);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nout = p.nout;
+  const int64_t rows = p.rows;
+  C* const out = p.out;
+  const C alpha = p.alpha, beta = p.beta;
+  const int ls = p.ls;
+  const C* const ls_in = p.ls_in;
+  const C* const ls_chi = p.ls_chi;
+  const int64_t ls_chi_rs = p.ls_chi_rs;
+  const FDiv rows_rhs = p.rows_rhs, rows_zy = p.rows_zy;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const bool scatter = p.part_scatter != 0;
+  const int ty = p.ty, tz = p.tz, parT = p.parT;
+  const int d0 = p.tdiv[0], d1 = p.tdiv[1], d2 = p.tdiv[2];
+  const int64_t f0 = p.full[0], f1 = p.full[1], f2 = p.full[2];
+  const int(*toff)[3] = p.toff;
+  const int64_t g_off = p.g_off;
+  const C* const src = p.A + g0 * P;
+  auto gld = [=](int l, int i) -> C { return g0 + l < rows ? __ldcs(src + (int64_t)l * P + i) : czero<C>(); };
+  auto lds = [=](int l, int i) -> C { return sm[l * LS + i + (i >> 3)]; };
+  auto sts = [=](int l, int i, C v) { sm[l * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int l, int i, C v) {
+    const int64_t g = g0 + l;
+    if (g >= rows || i >= nout) return;
+    int64_t o;
+    const int64_t gg = g + g_off;
+    if (!scatter) {
+      o = gg * nout + i;
+    } else {
+      int64_t q = gg;
+      const int y = (int)(q % ty); q /= ty;
+      const int z = (int)(q % tz); q /= tz;
+      const int c = (int)(q % 3); q /= 3;
+      const int t = (int)(q % parT);
+      const int64_t rhs = q / parT;
+      const int64_t X = (int64_t)i * d0 + toff[t][0];
+      const int64_t Y = (int64_t)y * d1 + toff[t][1];
+      const int64_t Z = (int64_t)z * d2 + toff[t][2];
+      o = (((rhs * 3 + c) * f2 + Z) * f1 + Y) * f0 + X;
+    }
+    if (AXPBY)
+      out[o] = cadd(cmul(alpha, v), cmul(beta, out[o]));
+    else if (ls)
+      __stcs(out + o, ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, v));
+    else
+      __stcs(out + o, v);
+  };
+  ct_first_g<C, P, T, M, true, false, REV, false>(gld, sts);
+  __syncthreads();
+  ct_run_range<C, P, 1, 1, NST - 1, 8, T, M, true, false, REV>(p.tw, lds, lds, sts, sts, true, true);
+  ct_last_half<C, P, T, M, true, false, REV>(p.tw, lds, stg);
+}
+
+// FP32 x / y passes on line pairs with the global-fed first stage and the
+// half last stage of k_xfwd_g / k_y_g / k_xinv_g.
+template <int P, int T, int M2, bool INV, bool LF, bool REV, bool HALF, class GLd, class St>
+__device__ __forceinline__ void ct_first_g2(const GLd& gld, const St& st) {
+  constexpr int R = ct_radix_o<REV>(P, 0), TPL = P / R, NT = M2 * TPL, K = (NT + T - 1) / T;
+  constexpr int RIN = HALF ? R / 2 : R;
+  float2 a[K][R], b[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int lp = LF ? task % M2 : task / TPL, j = LF ? task / M2 : task % TPL;
+#pragma unroll
+      for (int r = 0; r < RIN; ++r) {
+        const float4 q = gld(lp, j + r * TPL);
+        a[k][r] = make_float2(q.x, q.y);
+        b[k][r] = make_float2(q.z, q.w);
+      }
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int lp = LF ? task % M2 : task / TPL, j = LF ? task / M2 : task % TPL;
+      if constexpr (HALF) {
+        bfly_half_in<R, INV>(a[k]);
+        bfly_half_in<R, INV>(b[k]);
+      } else {
+        Bfly<R, INV, float2>::run(a[k], nullptr, TPL);
+        Bfly<R, INV, float2>::run(b[k], nullptr, TPL);
+      }
+#pragma unroll
+      for (int r = 0; r < R; ++r) st(lp, j * R + r, make_float4(a[k][r].x, a[k][r].y, b[k][r].x, b[k][r].y));
+    }
+  }
+}
+
+template <int P, int T, int M2, bool INV, bool LF, bool REV, class Ld, class St>
+__device__ __forceinline__ void ct_last_half2(const float2* __restrict__ tw, const Ld& ld, const St& st) {
+  constexpr int S = ct_nst(P) - 1;
+  constexpr int R = ct_radix_o<REV>(P, S), NS = ct_span_o<REV>(P, S), TPL = P / R, NT = M2 * TPL;
+  constexpr int K = (NT + T - 1) / T, TWST = P / (NS * R);
+  static_assert(NS == TPL, "the last stage spans P / R");
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    if (NT % T == 0 || task < NT) {
+      const int lp = LF ? task % M2 : task / TPL, j = LF ? task / M2 : task % TPL;
+      float2 a[R], b[R];
+#pragma unroll
+      for (int r = 0; r < R; ++r) {
+        const float4 q = ld(lp, j + r * TPL);
+        a[r] = make_float2(q.x, q.y);
+        b[r] = make_float2(q.z, q.w);
+      }
+      float2 w[R];
+      twiddles<R, INV>(tw, j * TWST, w);
+#pragma unroll
+      for (int r = 1; r < R; ++r) {
+        a[r] = cmul(a[r], w[r]);
+        b[r] = cmul(b[r], w[r]);
+      }
+      bfly_half_out<R, INV>(a);
+      bfly_half_out<R, INV>(b);
+#pragma unroll
+      for (int r = 0; r < R / 2; ++r) st(lp, j + r * NS, make_float4(a[r].x, a[r].y, b[r].x, b[r].y));
+    }
+  }
+}
+
+template <int P, bool REV>
+__global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xfwd2_g(const XfParams<float2> p) {
+  constexpr int M = ct_xlines2<8>(P);
+  constexpr int M2 = M / 2;
+  constexpr int T = ct_threads2(M, P);
+  constexpr int LS = P + (P + 7) / 8;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int nin = p.nin;
+  const int64_t rows = p.rows;
+  float2* const A = p.A;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const float2* const src = p.in + g0 * nin;
+  const float2 z2 = make_float2(0.f, 0.f);
+  auto gld = [=](int lp, int i) -> float4 {
+    const bool in = i < nin;
+    const float2 u = (in && g0 + 2 * lp < rows) ? __ldcs(src + (int64_t)(2 * lp) * nin + i) : z2;
+    const float2 v = (in && g0 + 2 * lp + 1 < rows) ? __ldcs(src + (int64_t)(2 * lp + 1) * nin + i) : z2;
+    return make_float4(u.x, u.y, v.x, v.y);
+  };
+  auto lds = [=](int lp, int i) -> float4 { return sm[lp * LS + i + (i >> 3)]; };
+  auto sts = [=](int lp, int i, float4 v) { sm[lp * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int lp, int i, float4 v) {
+    const int64_t g = g0 + 2 * lp;
+    if (g < rows) A[g * P + i] = make_float2(v.x, v.y);
+    if (g + 1 < rows) A[(g + 1) * P + i] = make_float2(v.z, v.w);
+  };
+  ct_first_g2<P, T, M2, false, false, REV, true>(gld, sts);
+  __syncthreads();
+  ct_run_range2<P, 1, 1, ct_nst(P), T, M2, false, REV, false>(p.tw, lds, lds, sts, stg, true, false);
+}
+
+template <int P, bool REV>
+__global__ void __launch_bounds__(ct_threads2(ct_xlines2<8>(P), P)) k_xinv2_g(const XiParams<float2> p) {
+  constexpr int M = ct_xlines2<8>(P);
+  constexpr int M2 = M / 2;
+  constexpr int T = ct_threads2(M, P);
+  constexpr int LS = P + (P + 7) / 8;
+  constexpr int NST = ct_nst(P);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int nout = p.nout;
+  const int64_t rows = p.rows;
+  float2* const out = p.out;
+  const int64_t g0 = (int64_t)blockIdx.x * M;
+  const int64_t g_off = p.g_off;
+  const int ls = p.ls;
+  const float2* const ls_in = p.ls_in;
+  const float2* const ls_chi = p.ls_chi;
+  const int64_t ls_chi_rs = p.ls_chi_rs;
+  const FDiv rows_rhs = p.rows_rhs, rows_zy = p.rows_zy;
+  const float2* const src = p.A + g0 * P;
+  const float2 z2 = make_float2(0.f, 0.f);
+  auto gld = [=](int lp, int i) -> float4 {
+    const float2 u = g0 + 2 * lp < rows ? __ldcs(src + (int64_t)(2 * lp) * P + i) : z2;
+    const float2 v = g0 + 2 * lp + 1 < rows ? __ldcs(src + (int64_t)(2 * lp + 1) * P + i) : z2;
+    return make_float4(u.x, u.y, v.x, v.y);
+  };
+  auto lds = [=](int lp, int i) -> float4 { return sm[lp * LS + i + (i >> 3)]; };
+  auto sts = [=](int lp, int i, float4 v) { sm[lp * LS + i + (i >> 3)] = v; };
+  auto stg = [=](int lp, int i, float4 v) {
+    if (i >= nout) return;
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+      const int64_t g = g0 + 2 * lp + h;
+      if (g >= rows) return;
+      const int64_t gg = g + g_off;
+      const int64_t o = gg * nout + i;
+      const float2 w = h ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+      __stcs(out + o, ls ? ls_value(ls_in, ls_chi, ls_chi_rs, rows_rhs, rows_zy, nout, gg, i, o, w) : w);
+    }
+  };
+  ct_first_g2<P, T, M2, true, false, REV, false>(gld, sts);
+  __syncthreads();
+  ct_run_range2<P, 1, 1, NST - 1, T, M2, true, REV, false>(p.tw, lds, lds, sts, sts, true, true);
+  ct_last_half2<P, T, M2, true, false, REV>(p.tw, lds, stg);
+}
+
+template <int P, bool INV, int TX, bool REV>
+__global__ void __launch_bounds__(ct_threads2(TX, P), pow2_min_blocks(ct_threads2(TX, P), P)) k_y2_g(const YParams<float2> p) {
+  constexpr int T = ct_threads2(TX, P);
+  constexpr int M2 = TX / 2;
+  constexpr int NST = ct_nst(P);
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* const sm = reinterpret_cast<float4*>(smem_raw);
+  const int Px = p.Px, nin = p.nin, nout = p.nout;
+  const int tile = blockIdx.x % p.ntiles;
+  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int64_t rc = slice / p.nz;
+  const int z = (int)(slice % p.nz);
+  const int kx0 = tile * TX;
+  const float2* const src = p.src + ((rc * p.src_z + z) - p.src_sub) * p.src_rows * (int64_t)Px + kx0;
+  float2* const dst = p.dst + ((rc * p.dst_z + z) - p.dst_sub) * p.dst_rows * (int64_t)Px + kx0;
+  const int tmax = Px - kx0;  // even: Px and kx0 are even
+  auto gld = [=](int t2, int i) -> float4 {
+    return (2 * t2 < tmax && i < nin) ? __ldcs(reinterpret_cast<const float4*>(src + (int64_t)i * Px) + t2)
+                                      : make_float4(0.f, 0.f, 0.f, 0.f);
+  };
+  auto lds = [=](int t2, int i) -> float4 { return sm[i * M2 + t2]; };
+  auto sts = [=](int t2, int i, float4 v) { sm[i * M2 + t2] = v; };
+  auto stg = [=](int t2, int i, float4 v) {
+    if (2 * t2 < tmax && i < nout) {
+      float4* const q = reinterpret_cast<float4*>(dst + (int64_t)i * Px) + t2;
+      if constexpr (!INV)
+        __stcs(q, v);
+      else
+        *q = v;
+    }
+  };
+  if constexpr (!INV) {
+    ct_first_g2<P, T, M2, false, true, REV, true>(gld, sts);
+    __syncthreads();
+    ct_run_range2<P, 1, 1, NST, T, M2, false, REV, true>(p.tw, lds, lds, sts, stg, true, false);
+  } else {
+    ct_first_g2<P, T, M2, true, true, REV, false>(gld, sts);
+    __syncthreads();
+    ct_run_range2<P, 1, 1, NST - 1, T, M2, true, REV, true>(p.tw, lds, lds, sts, sts, true, true);
+    ct_last_half2<P, T, M2, true, true, REV>(p.tw, lds, stg);
   }
 }
 
@@ -1674,6 +2107,303 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf2_min_blo
   }
 }
 
+// ------------------------------------------------------------------------
+// FP32 fused z pass on line pairs, in the form of k_zg_ct: forward stage 0
+// fed from global memory with the zero padding pruned, middle stages with
+// twiddles shared by the three components and both lines of a pair, FMA-chain
+// multiply with sign-bit flips, and a last inverse stage that forms only the
+// target half.  Every tile width gives identical bits.
+
+__device__ __forceinline__ float2 cflip(float2 a, int f) {
+  const int m = (f != 0) << 31;
+  return make_float2(__int_as_float(__float_as_int(a.x) ^ m), __int_as_float(__float_as_int(a.y) ^ m));
+}
+
+__device__ __forceinline__ float2 mac3(const float2& g0, const float2& a, const float2& g1, const float2& b,
+                                      const float2& g2, const float2& c, float s) {
+  float re = g0.x * a.x;
+  re = fmaf(-g0.y, a.y, re);
+  re = fmaf(g1.x, b.x, re);
+  re = fmaf(-g1.y, b.y, re);
+  re = fmaf(g2.x, c.x, re);
+  re = fmaf(-g2.y, c.y, re);
+  float im = g0.x * a.y;
+  im = fmaf(g0.y, a.x, im);
+  im = fmaf(g1.x, b.y, im);
+  im = fmaf(g1.y, b.x, im);
+  im = fmaf(g2.x, c.y, im);
+  im = fmaf(g2.y, c.x, im);
+  return make_float2(re * s, im * s);
+}
+
+__device__ __forceinline__ void zmul3f(float2& x0, float2& x1, float2& x2, const float2 (&g)[6], int rx, int ry,
+                                       int rz, float s) {
+  const float2 gxy = cflip(g[3], rx ^ ry), gxz = cflip(g[4], rx ^ rz), gyz = cflip(g[5], ry ^ rz);
+  const float2 a = x0, b = x1, c = x2;
+  x0 = mac3(g[0], a, gxy, b, gxz, c, s);
+  x1 = mac3(gxy, a, g[1], b, gyz, c, s);
+  x2 = mac3(gxz, a, gyz, b, g[2], c, s);
+}
+
+// middle stage on line pairs (float4 = element q of lines 2 lp, 2 lp + 1)
+template <int P, int S, int T, int TX, bool INV, bool REV, class Slot>
+__device__ __forceinline__ void zg_mid2(float2* sm, const float2* __restrict__ tw, const Slot& slot) {
+  constexpr int R = ct_radix_o<REV>(P, S), NS = ct_span_o<REV>(P, S), TPL = P / R, M2 = TX / 2, NT = M2 * TPL;
+  constexpr int K = (NT + T - 1) / T, TWST = P / (NS * R), CH = P * TX;
+  float2 w[K][R];
+#pragma unroll
+  for (int k = 0; k < K; ++k) {
+    const int task = (int)threadIdx.x + k * T;
+    const int j = task / M2;
+    if (NS > 1) twiddles<R, INV>(tw, (j % NS) * TWST, w[k]);
+  }
+#pragma unroll 1
+  for (int c = 0; c < 3; ++c) {
+    float4* const smc = reinterpret_cast<float4*>(sm + c * CH);
+    float2 a[K][R], b[K][R];
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NT % T == 0 || task < NT) {
+        const int lp = task % M2, j = task / M2;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+          const float4 q = smc[slot(j + r * TPL) * M2 + lp];
+          a[k][r] = make_float2(q.x, q.y);
+          b[k][r] = make_float2(q.z, q.w);
+        }
+      }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      if (NT % T == 0 || task < NT) {
+        const int lp = task % M2, j = task / M2, jm = j % NS;
+        if (NS > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            a[k][r] = cmul(a[k][r], w[k][r]);
+            b[k][r] = cmul(b[k][r], w[k][r]);
+          }
+        }
+        Bfly<R, INV, float2>::run(a[k], tw, TPL);
+        Bfly<R, INV, float2>::run(b[k], tw, TPL);
+        const int base = (j - jm) * R + jm;
+#pragma unroll
+        for (int r = 0; r < R; ++r)
+          smc[(base + r * NS) * M2 + lp] = make_float4(a[k][r].x, a[k][r].y, b[k][r].x, b[k][r].y);
+      }
+    }
+  }
+}
+
+template <int P, int TX>
+__global__ void __launch_bounds__(ct_threads2(TX, P), zf2_min_blocks(ct_threads2(TX, P), P))
+    k_zg2_ct(const ZParams<float2> p) {
+  using C = float2;
+  constexpr int T = ct_threads2(TX, P);
+  constexpr int M2 = TX / 2;
+  constexpr int CH = P * TX;
+  constexpr int NST = ct_nst(P);
+  constexpr int RL = ct_radix(P, NST - 1);
+  constexpr int TPL = P / RL;
+  constexpr int TPL0 = P / 8, NT0 = M2 * TPL0, K0 = (NT0 + T - 1) / T;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* const sm = reinterpret_cast<C*>(smem_raw);
+  const int nrhs = p.nrhs, ntiles = p.ntiles, Px = p.Px, Py = p.Py;
+  const int nin = p.nin, nout = p.nout;
+  const int rhs = blockIdx.x % nrhs;
+  const int rest = blockIdx.x / nrhs;
+  const int tseq = rest % ntiles;
+  const int yseq = rest / ntiles;
+  const int kx0 = tile_seq(tseq, ntiles) * TX;
+  const int ky = mirror_seq(yseq, Py);
+  const int tmax = Px - kx0;  // even: Px and kx0 are even
+  const int64_t plane = (int64_t)Py * Px;
+  C* const Bb = p.B + (int64_t)rhs * 3 * p.zb * plane + (int64_t)ky * Px + kx0;
+  const C* const tw = p.tw;
+  // forward stage 0 (radix 8, span 1): pair task (lp, j0) reads z = j0 + r
+  // * TPL0, r < 4, as 16-byte loads of both lines
+  {
+    float2 a[3][K0][8], b[3][K0][8];
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        const int lp = task % M2, j0 = task / M2;
+        const bool ok = (NT0 % T == 0 || task < NT0) && 2 * lp < tmax;
+        const float4* const src = reinterpret_cast<const float4*>(Bb + (int64_t)c * nin * plane) + lp;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int i = j0 + r * TPL0;
+          const float4 q = (ok && i < nin) ? __ldcs(reinterpret_cast<const float4*>(
+                                                 reinterpret_cast<const C*>(src) + (int64_t)i * plane))
+                                           : make_float4(0.f, 0.f, 0.f, 0.f);
+          a[c][k][r] = make_float2(q.x, q.y);
+          b[c][k][r] = make_float2(q.z, q.w);
+        }
+      }
+#pragma unroll
+    for (int c = 0; c < 3; ++c)
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        if (NT0 % T == 0 || task < NT0) {
+          const int lp = task % M2, j0 = task / M2;
+          bfly8_half_in<false>(a[c][k]);
+          bfly8_half_in<false>(b[c][k]);
+          float4* const dst = reinterpret_cast<float4*>(sm + c * CH) + (j0 * 8) * M2 + lp;
+#pragma unroll
+          for (int r = 0; r < 8; ++r) dst[r * M2] = make_float4(a[c][k][r].x, a[c][k][r].y, b[c][k][r].x, b[c][k][r].y);
+        }
+      }
+  }
+  __syncthreads();
+  {
+    auto nat = [](int q) { return q; };
+    if constexpr (NST >= 3) zg_mid2<P, 1, T, TX, false, false>(sm, tw, nat);
+    if constexpr (NST >= 4) zg_mid2<P, 2, T, TX, false, false>(sm, tw, nat);
+    if constexpr (NST >= 5) zg_mid2<P, 3, T, TX, false, false>(sm, tw, nat);
+  }
+  int py, iy, ry;
+  ax_map(p.ax[1], ky, py, iy, ry);
+  const int tx = p.tx, ty = p.ty, tz = p.tz;
+  const float s = (float)p.scale;
+  const float4* const sm4 = reinterpret_cast<const float4*>(sm);
+  float4* const smw = reinterpret_cast<float4*>(sm);
+  {
+    constexpr int NTASK = M2 * TPL;
+    constexpr int K = (NTASK + T - 1) / T;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      const bool live = (NTASK % T == 0 || task < NTASK) && 2 * (task % M2) < tmax;
+      const int lp = task % M2, j = task / M2;
+      // the two columns kx0 + 2 lp (even parity) and kx0 + 2 lp + 1 (odd)
+      int pxa = 0, ixa = 0, rxa = 0, pxb = 0, ixb = 0, rxb = 0;
+      ax_map(p.ax[0], kx0 + 2 * lp, pxa, ixa, rxa);
+      ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+      // the first frequency's kernel values (both columns) go out before the barrier
+      C ga[6], gb[6];
+      int rz = 0;
+      if (live) {
+        int pz, iz;
+        ax_map(p.ax[2], j, pz, iz, rz);
+        const C* gpa = ker_at(p.ker, 4 * pxa + 2 * py + pz, iz, iy, ixa, tx, ty, tz);
+        const C* gpb = ker_at(p.ker, 4 * pxb + 2 * py + pz, iz, iy, ixb, tx, ty, tz);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          ga[q] = ker_ld(gpa, q, tx);
+          gb[q] = ker_ld(gpb, q, tx);
+        }
+      }
+      if (k == 0) __syncthreads();
+      if (!live) continue;
+      C a[3][RL], b[3][RL];
+#pragma unroll
+      for (int c = 0; c < 3; ++c)
+#pragma unroll
+        for (int r = 0; r < RL; ++r) {
+          const float4 q = sm4[(c * CH + (j + r * TPL) * TX) / 2 + lp];
+          a[c][r] = make_float2(q.x, q.y);
+          b[c][r] = make_float2(q.z, q.w);
+        }
+      {
+        C w[RL];
+        twiddles<RL, false>(tw, j, w);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+#pragma unroll
+          for (int r = 1; r < RL; ++r) {
+            a[c][r] = cmul(a[c][r], w[r]);
+            b[c][r] = cmul(b[c][r], w[r]);
+          }
+          Bfly<RL, false, C>::run(a[c], tw, TPL);
+          Bfly<RL, false, C>::run(b[c], tw, TPL);
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < RL; ++r) {
+        if (r > 0) {
+          int pz, iz;
+          ax_map(p.ax[2], j + r * TPL, pz, iz, rz);
+          const C* gpa = ker_at(p.ker, 4 * pxa + 2 * py + pz, iz, iy, ixa, tx, ty, tz);
+          const C* gpb = ker_at(p.ker, 4 * pxb + 2 * py + pz, iz, iy, ixb, tx, ty, tz);
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            ga[q] = ker_ld(gpa, q, tx);
+            gb[q] = ker_ld(gpb, q, tx);
+          }
+        }
+        zmul3f(a[0][r], a[1][r], a[2][r], ga, rxa, ry, rz, s);
+        zmul3f(b[0][r], b[1][r], b[2][r], gb, rxb, ry, rz, s);
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) {
+        Bfly<RL, true, C>::run(a[c], tw, TPL);
+        Bfly<RL, true, C>::run(b[c], tw, TPL);
+#pragma unroll
+        for (int r = 0; r < RL; ++r)
+          smw[(c * CH + (j + r * TPL) * TX) / 2 + lp] = make_float4(a[c][r].x, a[c][r].y, b[c][r].x, b[c][r].y);
+      }
+    }
+  }
+  __syncthreads();
+  {
+    auto perm = [](int q) { return (q / RL) + (q % RL) * TPL; };
+    auto nat = [](int q) { return q; };
+    if constexpr (NST >= 3) zg_mid2<P, 1, T, TX, true, true>(sm, tw, perm);
+    if constexpr (NST >= 4) zg_mid2<P, 2, T, TX, true, true>(sm, tw, nat);
+    if constexpr (NST >= 5) zg_mid2<P, 3, T, TX, true, true>(sm, tw, nat);
+  }
+  __syncthreads();
+  // inverse last stage (radix 8, span TPL0): the target half, straight to B
+  {
+    float2 w[K0][8];
+#pragma unroll
+    for (int k = 0; k < K0; ++k) {
+      const int task = (int)threadIdx.x + k * T;
+      twiddles<8, true>(tw, task / M2, w[k]);
+    }
+#pragma unroll 1
+    for (int c = 0; c < 3; ++c) {
+      const float4* const smc = reinterpret_cast<const float4*>(sm + c * CH);
+      C* const Bo = Bb + (int64_t)c * nout * plane;
+#pragma unroll
+      for (int k = 0; k < K0; ++k) {
+        const int task = (int)threadIdx.x + k * T;
+        if (NT0 % T == 0 || task < NT0) {
+          const int lp = task % M2, j = task / M2;
+          float2 a[8], b[8];
+#pragma unroll
+          for (int r = 0; r < 8; ++r) {
+            const float4 q = smc[(j + r * TPL0) * M2 + lp];
+            a[r] = make_float2(q.x, q.y);
+            b[r] = make_float2(q.z, q.w);
+          }
+#pragma unroll
+          for (int r = 1; r < 8; ++r) {
+            a[r] = cmul(a[r], w[k][r]);
+            b[r] = cmul(b[r], w[k][r]);
+          }
+          bfly8_half_out<true>(a);
+          bfly8_half_out<true>(b);
+          if (2 * lp < tmax) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+              const int i = j + r * TPL0;
+              if (i < nout)
+                __stcs(reinterpret_cast<float4*>(Bo + (int64_t)i * plane) + lp, make_float4(a[r].x, a[r].y, b[r].x, b[r].y));
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
 template <typename C, int P, bool AXPBY, bool REV>
 __global__ void __launch_bounds__(ct_threads(ct_xlines<sizeof(C)>(P), P)) k_xinv_ct(const XiParams<C> p) {
   constexpr int M = ct_xlines<sizeof(C)>(P);
@@ -1766,6 +2496,15 @@ static inline bool zgo() {
   }();
   return on;
 }
+// FP64 x / y passes with a global-fed first stage and a half last stage
+// (k_xfwd_g, k_y_g, k_xinv_g) where they apply (GILA_XYG=0: the staged ones)
+static inline bool xyg() {
+  static const bool on = [] {
+    const char* e = getenv("GILA_XYG");
+    return !(e && e[0] == '0');
+  }();
+  return on;
+}
 // two-stage FP64 z pass (k_zr_ct) where it applies (GILA_ZTWO=0: k_zf_ct)
 static inline bool ztwo() {
   static const bool on = [] {
@@ -1826,6 +2565,16 @@ static bool is_mixed(const AxisPlan& pl) {
     KERNEL<<<(unsigned)blocks, T, sm, st>>>(__VA_ARGS__);                                    \
   } while (0)
 
+// launch of an FP32 line-pair kernel with T threads (returns from the caller)
+#define GILA_LAUNCH2_SB(KERNEL, TT, SMB, NB, ARG)                  \
+  do {                                                          \
+    cudaError_t e__ = set_smem((const void*)KERNEL, SMB);       \
+    if (e__ != cudaSuccess) return e__;                         \
+    KERNEL<<<(unsigned)(NB), TT, SMB, st>>>(ARG);                \
+    return cudaGetLastError();                                  \
+  } while (0)
+#define GILA_LAUNCH2(KERNEL, TT, ARG) GILA_LAUNCH2_SB(KERNEL, TT, sm, blocks, ARG)
+
 // one launch of a compile-time x / y kernel in the chosen radix order
 template <int P, bool REV>
 static cudaError_t run_xfwd2(const XfParams<float2>& p, int T, size_t sm, int64_t blocks, cudaStream_t st) {
@@ -1871,6 +2620,17 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
       const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                         \
       p.M = M;                                                                         \
       const int64_t blocks = (p.rows + M - 1) / M;                                     \
+      if (xyg() && L.xy_g && 2 * p.nin <= n) {                                                   \
+        if (L.x_rev) {                                                                 \
+          if constexpr (xyg_in_ok<n, true>()) {                                        \
+            GILA_LAUNCH2((k_xfwd2_g<n, true>), T2, xfp32(p));                            \
+          }                                                                            \
+        } else {                                                                       \
+          if constexpr (xyg_in_ok<n, false>()) {                                       \
+            GILA_LAUNCH2((k_xfwd2_g<n, false>), T2, xfp32(p));                           \
+          }                                                                            \
+        }                                                                              \
+      }                                                                                \
       return L.x_rev ? run_xfwd2<n, true>(xfp32(p), T2, sm, blocks, st)               \
                      : run_xfwd2<n, false>(xfp32(p), T2, sm, blocks, st);             \
     }                                                                                  \
@@ -1881,6 +2641,21 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
     const size_t sm = (size_t)M * row_stride(n) * sizeof(C);                           \
     p.M = M;                                                                           \
     const int64_t blocks = (p.rows + M - 1) / M;                                       \
+    if constexpr (sizeof(C) == 16) {                                                   \
+      if (xyg() && L.xy_g && 2 * p.nin <= n) {                                                   \
+        if (L.x_rev) {                                                                 \
+          if constexpr (xyg_in_ok<n, true>()) {                                        \
+            GILA_LAUNCH(false, (k_xfwd_g<n, true>), p);                                \
+            return cudaGetLastError();                                                 \
+          }                                                                            \
+        } else {                                                                       \
+          if constexpr (xyg_in_ok<n, false>()) {                                       \
+            GILA_LAUNCH(false, (k_xfwd_g<n, false>), p);                               \
+            return cudaGetLastError();                                                 \
+          }                                                                            \
+        }                                                                              \
+      }                                                                                \
+    }                                                                                  \
     if (L.x_rev)                                                                       \
       GILA_LAUNCH(false, (k_xfwd_ct<C, n, true>), p);                                  \
     else                                                                               \
@@ -1902,7 +2677,7 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
 }
 
 template <typename C, bool INV>
-static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, bool rev,
+static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, bool rev, bool gform,
                                 cudaStream_t st) {
   if (ct_has(p.P)) {
 #define GILA_CT_Y2(n, tx)                                  \
@@ -1911,10 +2686,36 @@ static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, 
       if constexpr (sizeof(C) == 8) {                      \
         if (zpair()) {                                     \
           const int T2 = ct_threads2(tx, n);               \
+          if (xyg() && gform && (INV ? 2 * p.nout <= n : 2 * p.nin <= n)) { \
+            if (rev) {                                     \
+              if constexpr (INV ? xyg_out_ok<n, true>() : xyg_in_ok<n, true>()) { \
+                GILA_LAUNCH2((k_y2_g<n, INV, tx, true>), T2, yp32(p)); \
+              }                                            \
+            } else {                                       \
+              if constexpr (INV ? xyg_out_ok<n, false>() : xyg_in_ok<n, false>()) { \
+                GILA_LAUNCH2((k_y2_g<n, INV, tx, false>), T2, yp32(p)); \
+              }                                            \
+            }                                              \
+          }                                                \
           return rev ? run_y2<n, INV, tx, true>(yp32(p), T2, sm, blocks, st) \
                      : run_y2<n, INV, tx, false>(yp32(p), T2, sm, blocks, st); \
         }                                                  \
       }                                                    \
+      if constexpr (sizeof(C) == 16) {                                                 \
+        if (xyg() && gform && (INV ? 2 * p.nout <= n : 2 * p.nin <= n)) {                       \
+          if (rev) {                                                                   \
+            if constexpr (INV ? xyg_out_ok<n, true>() : xyg_in_ok<n, true>()) {        \
+              GILA_LAUNCH(false, (k_y_g<n, INV, tx, true>), p);                        \
+              return cudaSuccess;                                                      \
+            }                                                                          \
+          } else {                                                                     \
+            if constexpr (INV ? xyg_out_ok<n, false>() : xyg_in_ok<n, false>()) {      \
+              GILA_LAUNCH(false, (k_y_g<n, INV, tx, false>), p);                       \
+              return cudaSuccess;                                                      \
+            }                                                                          \
+          }                                                                            \
+        }                                                                              \
+      }                                                                                \
       if (rev)                                             \
         GILA_LAUNCH(false, (k_y_ct<C, n, INV, tx, true>), p); \
       else                                                 \
@@ -1977,8 +2778,8 @@ cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv
   const size_t sm = (size_t)p.TX * p.P * sizeof(C);
   const bool mx = is_mixed(d.plan[1]);
   const int64_t blocks = (int64_t)p.ntiles * nq;
-  cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, L.y_rev != 0, st)
-                      : launch_y_one<C, false>(p, mx, T, sm, blocks, L.y_rev != 0, st);
+  cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, L.y_rev != 0, L.xy_g != 0, st)
+                      : launch_y_one<C, false>(p, mx, T, sm, blocks, L.y_rev != 0, L.xy_g != 0, st);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }
@@ -2043,6 +2844,16 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
       }                                               \
       if constexpr (zf_ok(sizeof(C), n)) {            \
         if (p.parT == 1 && zfuse()) {                 \
+          if constexpr (sizeof(C) == 8 && zg_ok<n>()) { \
+            if (zpair() && zgo() && 2 * p.nin <= n && 2 * p.nout <= n) { \
+              const int T2 = ct_threads2(tx, n);      \
+              const void* fn2 = (const void*)k_zg2_ct<n, tx>; \
+              cudaError_t e2 = set_smem(fn2, sm);     \
+              if (e2 != cudaSuccess) return e2;       \
+              k_zg2_ct<n, tx><<<(unsigned)blocks, T2, sm, st>>>(zp32(p)); \
+              return cudaGetLastError();              \
+            }                                         \
+          }                                           \
           if constexpr (sizeof(C) == 8) {             \
             if (zpair()) {                            \
               const int T2 = ct_threads2(tx, n);      \
@@ -2076,7 +2887,7 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
 
 template <typename C, bool AXPBY>
 static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t sm, int64_t blocks, bool rev,
-                                   cudaStream_t st) {
+                                   bool gform, cudaStream_t st) {
   if (ct_has(p.P)) {
 #define GILA_CT_XI(n)                                                    \
   if constexpr (sizeof(C) == 8 && !AXPBY) {                              \
@@ -2085,11 +2896,37 @@ static cudaError_t launch_xinv_one(const XiParams<C>& p, bool mx, int T, size_t 
       const int T2 = ct_threads2(M2r, n);                                \
       const size_t sm2 = (size_t)M2r * row_stride(n) * sizeof(C);        \
       const int64_t blocks2 = (p.rows + M2r - 1) / M2r;                  \
+      if (xyg() && gform && 2 * p.nout <= n) {                                  \
+        if (rev) {                                                     \
+          if constexpr (xyg_out_ok<n, true>()) {                       \
+            GILA_LAUNCH2_SB((k_xinv2_g<n, true>), T2, sm2, blocks2, xip32(p)); \
+          }                                                            \
+        } else {                                                       \
+          if constexpr (xyg_out_ok<n, false>()) {                      \
+            GILA_LAUNCH2_SB((k_xinv2_g<n, false>), T2, sm2, blocks2, xip32(p)); \
+          }                                                            \
+        }                                                              \
+      }                                                                \
       return rev ? run_xinv2<n, true>(xip32(p), T2, sm2, blocks2, st)    \
                  : run_xinv2<n, false>(xip32(p), T2, sm2, blocks2, st);  \
     }                                                                    \
   }                                                                      \
   if (p.P == n) {                                                        \
+    if constexpr (sizeof(C) == 16) {                                                   \
+      if (xyg() && gform && 2 * p.nout <= n) {                                                  \
+        if (rev) {                                                                     \
+          if constexpr (xyg_out_ok<n, true>()) {                                       \
+            GILA_LAUNCH(false, (k_xinv_g<n, AXPBY, true>), p);                         \
+            return cudaSuccess;                                                        \
+          }                                                                            \
+        } else {                                                                       \
+          if constexpr (xyg_out_ok<n, false>()) {                                      \
+            GILA_LAUNCH(false, (k_xinv_g<n, AXPBY, false>), p);                        \
+            return cudaSuccess;                                                        \
+          }                                                                            \
+        }                                                                              \
+      }                                                                                \
+    }                                                                                  \
     if (rev)                                                             \
       GILA_LAUNCH(false, (k_xinv_ct<C, n, AXPBY, true>), p);             \
     else                                                                 \
@@ -2154,8 +2991,8 @@ cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const
   const bool mx = is_mixed(d.plan[0]);
   const int64_t blocks = (p.rows + p.M - 1) / p.M;
   cudaError_t e =
-      axpby ? launch_xinv_one<C, true>(p, mx, T, sm, blocks, L.x_rev != 0, st)
-            : launch_xinv_one<C, false>(p, mx, T, sm, blocks, L.x_rev != 0, st);
+      axpby ? launch_xinv_one<C, true>(p, mx, T, sm, blocks, L.x_rev != 0, L.xy_g != 0, st)
+            : launch_xinv_one<C, false>(p, mx, T, sm, blocks, L.x_rev != 0, L.xy_g != 0, st);
   if (e != cudaSuccess) return e;
   return cudaGetLastError();
 }

@@ -1410,7 +1410,7 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   so.tol = opts && opts->tol > 0 ? opts->tol : 1e-6;
   so.max_mv = opts && opts->max_matvecs > 0 ? opts->max_matvecs : 4000;
   so.max_restarts = opts && opts->max_restarts > 0 ? opts->max_restarts : 20;
-  so.delta = opts && opts->delta > 0 ? opts->delta : 0.1;
+  so.delta = opts && opts->delta > 0 ? opts->delta : 0.01;
   so.x0 = opts ? (opts->x0 != 0) : 0;
   if (cfg.ell > 4) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
   Core* inner = nullptr;

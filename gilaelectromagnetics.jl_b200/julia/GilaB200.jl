@@ -319,7 +319,7 @@ function solve(ls::LippmannSchwinger, i::AbstractArray{ComplexF64}; tol=1e-6, mi
     n = 3 * prod(glaSze(ls.greens_op, 1)[1:3])
     nrhs = length(i) ÷ n
     b = Array(i); x = similar(b)
-    opts = Ref(CSolveOpts(tol, ell, mixed, max_matvecs, 0, 0.1, 0, 0, keep))
+    opts = Ref(CSolveOpts(tol, ell, mixed, max_matvecs, 0, 0.0, 0, 0, keep))  # delta 0: the library default
     info = Ref{CSolveInfo}()
     G32 = mixed ? g32(ls).h : C_NULL
     check(ccall((:gila_ls_solve, LIB), Cint,
