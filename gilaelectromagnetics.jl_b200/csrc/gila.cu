@@ -241,6 +241,16 @@ Core::~Core() {
   for (int k = 0; k < 2; ++k)
     for (cudaEvent_t x : {ev_in_ready[k], ev_in_free[k], ev_out_ready[k], ev_out_free[k]})
       if (x) cudaEventDestroy(x);
+  for (cudaStream_t x : pipe_st)
+    if (x) {
+      cudaStreamSynchronize(x);
+      cudaStreamDestroy(x);
+    }
+  for (int k = 0; k < kMaxKxChunks; ++k) {
+    if (pipe_ev_y[k]) cudaEventDestroy(pipe_ev_y[k]);
+    if (pipe_ev_z[k]) cudaEventDestroy(pipe_ev_z[k]);
+  }
+  if (pipe_join) cudaEventDestroy(pipe_join);
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -369,6 +379,12 @@ gila_status init_core(gila_ctx* ctx, const gila_vol* trg_abi, const gila_vol* sr
   GILA_CUDA_TRY(dev_malloc(&core->plan_d, 3 * sizeof(AxisPlan)));
   GILA_CUDA_TRY(cudaMemcpy(core->plan_d, core->plan, 3 * sizeof(AxisPlan), cudaMemcpyHostToDevice));
   GILA_CUDA_TRY(cudaStreamCreateWithFlags(&core->stream, cudaStreamNonBlocking));
+  for (int k = 0; k < 2; ++k) GILA_CUDA_TRY(cudaStreamCreateWithFlags(&core->pipe_st[k], cudaStreamNonBlocking));
+  for (int k = 0; k < kMaxKxChunks; ++k) {
+    GILA_CUDA_TRY(cudaEventCreateWithFlags(&core->pipe_ev_y[k], cudaEventDisableTiming));
+    GILA_CUDA_TRY(cudaEventCreateWithFlags(&core->pipe_ev_z[k], cudaEventDisableTiming));
+  }
+  GILA_CUDA_TRY(cudaEventCreateWithFlags(&core->pipe_join, cudaEventDisableTiming));
   return GILA_OK;
 }
 
@@ -1370,9 +1386,13 @@ gila_status gila_opr_device_bytes(const gila_opr* opr, int64_t* bytes) {
 
 gila_status gila_opr_launches_per_apply(const gila_opr* opr, int64_t nrhs, int64_t* n) {
   if (!opr || !n || nrhs < 1) return fail(GILA_ERR_ARG, "invalid argument");
-  Geom g = opr->core->geom;
+  const Core& c = *opr->core;
+  Geom g = c.geom;
   if (nrhs > g.max_rhs) g.max_rhs = (int)nrhs;
-  *n = matvec_launches(g, (int)nrhs);
+  const Launch L = c.tuned ? c.launch : default_launch(c);
+  const int nch = c.dtype == GILA_C128 ? kx_chunks<double2>(g, devop<double2>(c), L, (int)nrhs)
+                                       : kx_chunks<float2>(g, devop<float2>(c), L, (int)nrhs);
+  *n = matvec_launches(g, (int)nrhs, nch);
   return GILA_OK;
 }
 

@@ -94,6 +94,12 @@ struct Core {
   int64_t tuned_rhs = 0;  // batch size c.launch was picked for
   bool pinned = false;    // launch shapes forced by the caller (set_tiles / set_schedule)
   cudaStream_t stream = nullptr;
+  // the kx-chunk pipeline of the matvec (matvec.cuh): z-pass and inverse-y
+  // streams and their events, made with the operator so that no apply or
+  // stream capture creates any
+  cudaStream_t pipe_st[2] = {nullptr, nullptr};
+  cudaEvent_t pipe_ev_y[kMaxKxChunks] = {}, pipe_ev_z[kMaxKxChunks] = {};
+  cudaEvent_t pipe_join = nullptr;
   std::mutex mu;
   // a solve batch kept resident between gila_ls_solve calls (opts->keep)
   std::shared_ptr<LsBatch> ls_keep;
@@ -142,6 +148,13 @@ inline DevOp<C> devop(const Core& c) {
     d.plan_d[k] = c.plan_d + k;
   }
   d.scale = 1.0 / ((double)c.geom.P[0] * c.geom.P[1] * c.geom.P[2]);
+  d.pst[0] = c.pipe_st[0];
+  d.pst[1] = c.pipe_st[1];
+  for (int k = 0; k < kMaxKxChunks; ++k) {
+    d.pev_y[k] = c.pipe_ev_y[k];
+    d.pev_z[k] = c.pipe_ev_z[k];
+  }
+  d.pjoin = c.pipe_join;
   return d;
 }
 gila_status plan_axis(int P, AxisPlan* pl);

@@ -68,7 +68,8 @@ int pass_threads(const AxisPlan& pl, int M) {
 // The x and y passes run slab by slab over planes (ch, z) so that the slab
 // buffer A between them stays resident in L2 and is overwritten there by the
 // next slab: the x<->y intermediate then never reaches HBM.
-int64_t matvec_launches(const Geom& g, int nrhs) {
+int64_t matvec_launches(const Geom& g, int nrhs, int kx_chunks) {
+  if (kx_chunks > 1) return 2 + 3LL * kx_chunks;
   const Work w = work_sizes(g);
   const int64_t fwd_planes = 3LL * g.sc[2], inv_planes = 3LL * g.parT * g.tc[2];
   const bool fwd_flat = (int64_t)w.zb == g.sc[2];

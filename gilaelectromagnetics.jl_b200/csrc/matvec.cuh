@@ -53,6 +53,18 @@ constexpr int kEm = GILA_KE_MIXED;
 constexpr int kSlabBytes = 1 << 30;
 Work work_sizes(const Geom& g);
 
+// The y passes and the z pass of a self operator work on independent sets of
+// kx columns, so a matvec can run them as a pipeline over kx chunks: the z
+// pass of chunk c (bound by the L1 / shared-memory pipe) on its own stream
+// while the y passes of chunks c + 1 (forward) and c - 1 (inverse) run on
+// two others (bound by memory latency).  A chunk is a range of positions of
+// the z pass's mirror tile order (z tiles i and ntiles - 1 - i side by side).
+constexpr int kMaxKxChunks = 16;
+struct KxChunk {
+  int ts0 = 0;   // first position (even)
+  int nts = -1;  // positions; < 0: all
+};
+
 // Per-axis plan (radix list), twiddle tables and kernel-address maps live on
 // the device; Dev bundles the pointers for one dtype.
 template <typename C>
@@ -63,6 +75,12 @@ struct DevOp {
   AxisPlan plan[3];          // host copies (launch decisions)
   const AxisPlan* plan_d[3]; // device copies (read by the kernels)
   double scale;      // 1 / (Px Py Pz)
+  // the operator's kx-chunk pipeline: z-pass and inverse-y streams, per-chunk
+  // events after the forward y pass and after the z pass, the join event
+  // (no pipeline when pst[0] is null)
+  cudaStream_t pst[2] = {nullptr, nullptr};
+  cudaEvent_t pev_y[kMaxKxChunks] = {}, pev_z[kMaxKxChunks] = {};
+  cudaEvent_t pjoin = nullptr;
 };
 
 // Tile / launch parameters picked by the autotuner.
@@ -99,17 +117,23 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
                         cudaStream_t st);
 template <typename C>
 cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int64_t q0,
-                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st);
+                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st, const KxChunk* ch = nullptr);
 template <typename C>
-cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st);
+cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st,
+                     const KxChunk* ch = nullptr);
+// kx chunks the pipelined matvec uses for this operator and launch shape
+// (0: no pipeline)
+template <typename C>
+int kx_chunks(const Geom& g, const DevOp<C>& d, const Launch& L, int nrhs);
 template <typename C>
 cudaError_t launch_xinv(const Geom& g, const DevOp<C>& d, const Launch& L, const C* A, C* out, int64_t rows,
                         int64_t g_off, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls = nullptr);
 
 int smem_optin_bytes();
 
-// Kernels one matvec of nrhs vectors launches.
-int64_t matvec_launches(const Geom& g, int nrhs);
+// Kernels one matvec of nrhs vectors launches (kx_chunks > 1: the
+// pipelined form).
+int64_t matvec_launches(const Geom& g, int nrhs, int kx_chunks = 0);
 
 // The three phases of launch_matvec, for timing: forward x/y slabs, z pass,
 // inverse y/x slabs.

@@ -86,6 +86,9 @@ struct YParams {
   int64_t q0;                // first plane (ch*nz + z) of this launch
   int64_t src_sub, dst_sub;  // plane index of the first plane held by src / dst
   FDiv md;                   // division by the line count TX
+  // kx tiles of this launch: nt tiles, the first nlo from lo0 on, the rest
+  // from hi0 on (all tiles: nt = nlo = ntiles, lo0 = 0)
+  int nt, nlo, lo0, hi0;
 };
 
 template <typename C, bool INV, bool MX>
@@ -94,8 +97,9 @@ __global__ void __launch_bounds__(512) k_y(const YParams<C> p) {
   C* const sm = reinterpret_cast<C*>(smem_raw);
   const AxisPlan* const pl = p.pl;
   const int Px = p.Px, TX = p.TX, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int tl = blockIdx.x % p.nt;  // tile of the kx set: low range, then high range
+  const int tile = tl < p.nlo ? p.lo0 + tl : p.hi0 + (tl - p.nlo);
+  const int64_t slice = p.q0 + blockIdx.x / p.nt;  // ch*nz + z
   const int64_t rc = slice / p.nz;
   const int z = (int)(slice % p.nz);
   const int kx0 = tile * TX;
@@ -170,6 +174,7 @@ struct ZParams {
   FDiv md;    // division by the tile width TX
   FDiv nind;  // division by nin
   AxMap ax[3];
+  int ts0, nts;  // positions [ts0, ts0 + nts) of the mirror tile order (all: 0, ntiles)
 };
 
 // ky order that places each frequency next to its mirror Py - ky, and kx
@@ -218,8 +223,8 @@ __global__ void __launch_bounds__(512) k_z(const ZParams<C> p) {
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;
@@ -552,8 +557,9 @@ __global__ void __launch_bounds__(ct_threads(TX, P), pow2_min_blocks(ct_threads(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* const sm = reinterpret_cast<C*>(smem_raw);
   const int Px = p.Px, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int tl = blockIdx.x % p.nt;  // tile of the kx set: low range, then high range
+  const int tile = tl < p.nlo ? p.lo0 + tl : p.hi0 + (tl - p.nlo);
+  const int64_t slice = p.q0 + blockIdx.x / p.nt;  // ch*nz + z
   const int64_t rc = slice / p.nz;
   const int z = (int)(slice % p.nz);
   const int kx0 = tile * TX;
@@ -588,8 +594,9 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), pow2_min_blocks(ct_threads
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* const sm = reinterpret_cast<float4*>(smem_raw);
   const int Px = p.Px, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int tl = blockIdx.x % p.nt;  // tile of the kx set: low range, then high range
+  const int tile = tl < p.nlo ? p.lo0 + tl : p.hi0 + (tl - p.nlo);
+  const int64_t slice = p.q0 + blockIdx.x / p.nt;  // ch*nz + z
   const int64_t rc = slice / p.nz;
   const int z = (int)(slice % p.nz);
   const int kx0 = tile * TX;
@@ -626,8 +633,8 @@ __global__ void __launch_bounds__(ct_threads(TX, P)) k_z_ct(const ZParams<C> p) 
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;
@@ -788,8 +795,8 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;
@@ -991,8 +998,8 @@ __global__ void __launch_bounds__(zr_threads(TX, P), zr_min_blocks(zr_threads(TX
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;
@@ -1301,8 +1308,8 @@ __global__ void __launch_bounds__(ct_threads(TX, P), zf_min_blocks(ct_threads(TX
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;
@@ -1674,8 +1681,9 @@ __global__ void __launch_bounds__(ct_threads(TX, P), pow2_min_blocks(ct_threads(
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* const sm = reinterpret_cast<C*>(smem_raw);
   const int Px = p.Px, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int tl = blockIdx.x % p.nt;  // tile of the kx set: low range, then high range
+  const int tile = tl < p.nlo ? p.lo0 + tl : p.hi0 + (tl - p.nlo);
+  const int64_t slice = p.q0 + blockIdx.x / p.nt;  // ch*nz + z
   const int64_t rc = slice / p.nz;
   const int z = (int)(slice % p.nz);
   const int kx0 = tile * TX;
@@ -1927,8 +1935,9 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), pow2_min_blocks(ct_threads
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* const sm = reinterpret_cast<float4*>(smem_raw);
   const int Px = p.Px, nin = p.nin, nout = p.nout;
-  const int tile = blockIdx.x % p.ntiles;
-  const int64_t slice = p.q0 + blockIdx.x / p.ntiles;  // ch*nz + z
+  const int tl = blockIdx.x % p.nt;  // tile of the kx set: low range, then high range
+  const int tile = tl < p.nlo ? p.lo0 + tl : p.hi0 + (tl - p.nlo);
+  const int64_t slice = p.q0 + blockIdx.x / p.nt;  // ch*nz + z
   const int64_t rc = slice / p.nz;
   const int z = (int)(slice % p.nz);
   const int kx0 = tile * TX;
@@ -1993,8 +2002,8 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf2_min_blo
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;  // even: Px and kx0 are even
@@ -2215,8 +2224,8 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), zf2_min_blocks(ct_threads2
   const int nin = p.nin, nout = p.nout;
   const int rhs = blockIdx.x % nrhs;
   const int rest = blockIdx.x / nrhs;
-  const int tseq = rest % ntiles;
-  const int yseq = rest / ntiles;
+  const int tseq = p.ts0 + rest % p.nts;  // [ts0, ts0 + nts) of the mirror tile order
+  const int yseq = rest / p.nts;
   const int kx0 = tile_seq(tseq, ntiles) * TX;
   const int ky = mirror_seq(yseq, Py);
   const int tmax = Px - kx0;  // even: Px and kx0 are even
@@ -2739,9 +2748,25 @@ static cudaError_t launch_y_one(const YParams<C>& p, bool mx, int T, size_t sm, 
 // One y pass over planes [q0, q0 + nq) (plane = ch*nz + z) of one rhs.
 // Forward: src = x-pass slab holding planes from src_sub on, dst = B of the
 // rhs.  Inverse: src = B of the rhs, dst = slab holding planes from dst_sub.
+// y tile ranges of a kx chunk: positions [ts0, ts0 + nts) of the z pass's
+// mirror tile order are z tiles p0 .. p1 - 1 and ntz - p1 .. ntz - p0 - 1
+// (p = ts0 / 2 ...), i.e. the kx ranges [p0 txz, p1 txz) and [Px - p1 txz,
+// Px - p0 txz); false when they do not fall on y tile boundaries
+static bool chunk_y_tiles(int Px, int txz, int txy, const KxChunk& ch, int& lo0, int& nlo, int& hi0, int& nt) {
+  if (txz <= 0 || txy <= 0 || Px % txz || Px % txy || (Px / txz) % 2 || ch.ts0 % 2 || ch.nts % 2) return false;
+  const int p0 = ch.ts0 / 2, p1 = (ch.ts0 + ch.nts) / 2;
+  const int k0 = p0 * txz, k1 = p1 * txz;
+  if (k0 % txy || k1 % txy || 2 * k1 > Px) return false;
+  lo0 = k0 / txy;
+  nlo = (k1 - k0) / txy;
+  hi0 = (Px - k1) / txy;
+  nt = 2 * nlo;
+  return true;
+}
+
 template <typename C>
 cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int64_t q0,
-                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st) {
+                     int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st, const KxChunk* ch) {
   YParams<C> p;
   p.src = src;
   p.dst = dst;
@@ -2773,11 +2798,17 @@ cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv
   if (ct_has(p.P)) p.TX = ct_tile_pick(sizeof(C), p.P, L.y_tx, false);
   p.ntiles = (p.Px + p.TX - 1) / p.TX;
   p.md = make_fdiv((uint32_t)p.TX);
+  p.nt = p.nlo = p.ntiles;
+  p.lo0 = p.hi0 = 0;
+  if (ch && ch->nts >= 0) {
+    const int txz = ct_has(g.P[2]) ? ct_tile_pick(sizeof(C), g.P[2], L.z_tx, true) : L.z_tx;
+    if (!chunk_y_tiles(p.Px, txz, p.TX, *ch, p.lo0, p.nlo, p.hi0, p.nt)) return cudaErrorInvalidValue;
+  }
   const int T = ct_has(p.P) ? ct_threads(p.TX, p.P) : pass_threads(d.plan[1], p.TX);
   if (T > 512) return cudaErrorInvalidConfiguration;
   const size_t sm = (size_t)p.TX * p.P * sizeof(C);
   const bool mx = is_mixed(d.plan[1]);
-  const int64_t blocks = (int64_t)p.ntiles * nq;
+  const int64_t blocks = (int64_t)p.nt * nq;
   cudaError_t e = inv ? launch_y_one<C, true>(p, mx, T, sm, blocks, L.y_rev != 0, L.xy_g != 0, st)
                       : launch_y_one<C, false>(p, mx, T, sm, blocks, L.y_rev != 0, L.xy_g != 0, st);
   if (e != cudaSuccess) return e;
@@ -2785,7 +2816,8 @@ cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv
 }
 
 template <typename C>
-cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st) {
+cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st,
+                     const KxChunk* ch) {
   const Work w = work_sizes(g);
   ZParams<C> p;
   p.B = B;
@@ -2819,10 +2851,17 @@ cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, in
   p.ntiles = (p.Px + p.TX - 1) / p.TX;
   p.md = make_fdiv((uint32_t)p.TX);
   p.nind = make_fdiv((uint32_t)p.nin);
+  p.ts0 = 0;
+  p.nts = p.ntiles;
+  if (ch && ch->nts >= 0) {
+    if (ch->ts0 < 0 || ch->ts0 + ch->nts > p.ntiles) return cudaErrorInvalidValue;
+    p.ts0 = ch->ts0;
+    p.nts = ch->nts;
+  }
   const int T = ct_has(p.P) ? ct_threads(p.TX, p.P) : pass_threads(d.plan[2], p.TX);
   if (T > 512) return cudaErrorInvalidConfiguration;
   const size_t sm = (size_t)3 * p.TX * p.P * sizeof(C) * (g.parT > 1 ? 2 : 1);
-  const int64_t blocks = (int64_t)p.ntiles * p.Py * nrhs;
+  const int64_t blocks = (int64_t)p.nts * p.Py * nrhs;
   if (ct_has(p.P)) {
 #define GILA_CT_Z2(n, tx)                             \
   if constexpr (ct_z_ok(sizeof(C), n, tx)) {          \
@@ -3036,9 +3075,79 @@ cudaError_t launch_matvec_phase(int phase, const Geom& g, const DevOp<C>& d, con
   return cudaSuccess;
 }
 
+// kx chunks of the pipelined matvec (GILA_KX_CHUNKS sets the count; off by
+// default: at 256x256x128 F64 one apply took 3.34 ms unpipelined and 3.39 /
+// 3.43 / 3.49 ms with 2 / 4 / 8 chunks, F32 1.80 vs 1.84-1.91 ms -- the z
+// pass and the y passes contend for the same L1 / shared-memory pipe, and
+// the smaller launches lose tail efficiency and the kernel's L2 reuse):
+// self operators with specialised y / z lengths, one target partition, the
+// x/y slab holding every plane of every vector, chunk boundaries on both
+// tile widths
+static inline int kx_chunks_wanted() {
+  static const int n = [] {
+    const char* e = getenv("GILA_KX_CHUNKS");
+    const int v = e ? atoi(e) : 0;
+    return v < 0 ? 0 : (v > kMaxKxChunks ? kMaxKxChunks : v);
+  }();
+  return n;
+}
+
+template <typename C>
+int kx_chunks(const Geom& g, const DevOp<C>& d, const Launch& L, int nrhs) {
+  const int want = kx_chunks_wanted();
+  if (want < 2 || !d.pst[0] || !d.pst[1] || !d.pjoin || g.parT != 1) return 0;
+  if (!ct_has(g.P[1]) || !ct_has(g.P[2])) return 0;
+  const Work w = work_sizes(g);
+  const int64_t fwd = 3LL * g.sc[2] * nrhs, inv = 3LL * g.tc[2] * nrhs;
+  if ((int64_t)w.zb != g.sc[2] || (int64_t)w.zb != g.tc[2] || w.slab_planes < fwd || w.slab_planes < inv) return 0;
+  const int txz = ct_tile_pick(sizeof(C), g.P[2], L.z_tx, true);
+  const int txy = ct_tile_pick(sizeof(C), g.P[1], L.y_tx, false);
+  const int Px = g.P[0];
+  if (Px % txz || Px % txy || (Px / txz) % 2) return 0;
+  const int pairs = Px / txz / 2;
+  const int q = txy > txz ? txy / txz : 1;  // pairs per chunk boundary step
+  int n = want;
+  while (n > 1 && (pairs % n || (pairs / n) % q)) --n;
+  return n > 1 ? n : 0;
+}
+
+// The pipelined matvec: x forward on st; per kx chunk c the forward y pass
+// on st, the z pass on pst[0] after it, the inverse y pass on pst[1] after
+// that; x inverse on st after the last inverse y pass.  Chunks touch
+// disjoint kx columns of A and B, so the passes of different chunks run
+// concurrently; stream capture records the same dependencies.
+template <typename C>
+static cudaError_t launch_matvec_pipe(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A,
+                                      C* B, int nrhs, bool axpby, C alpha, C beta, cudaStream_t st,
+                                      const LsEpi<C>* ls, int nch) {
+  cudaError_t e;
+  const int64_t fwd_planes = 3LL * g.sc[2] * nrhs, inv_planes = 3LL * g.tc[2] * nrhs;
+  const int txz = ct_tile_pick(sizeof(C), g.P[2], L.z_tx, true);
+  const int pairs = g.P[0] / txz / 2;
+  if ((e = launch_xfwd<C>(g, d, L, in, A, fwd_planes * g.sc[1], st)) != cudaSuccess) return e;
+  for (int c = 0; c < nch; ++c) {
+    KxChunk ch;
+    ch.ts0 = 2 * (pairs / nch) * c;
+    ch.nts = 2 * (pairs / nch);
+    if ((e = launch_y<C>(g, d, L, false, A, B, 0, fwd_planes, 0, 0, st, &ch)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(d.pev_y[c], st)) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(d.pst[0], d.pev_y[c], 0)) != cudaSuccess) return e;
+    if ((e = launch_z<C>(g, d, L, B, nrhs, d.pst[0], &ch)) != cudaSuccess) return e;
+    if ((e = cudaEventRecord(d.pev_z[c], d.pst[0])) != cudaSuccess) return e;
+    if ((e = cudaStreamWaitEvent(d.pst[1], d.pev_z[c], 0)) != cudaSuccess) return e;
+    if ((e = launch_y<C>(g, d, L, true, B, A, 0, inv_planes, 0, 0, d.pst[1], &ch)) != cudaSuccess) return e;
+  }
+  if ((e = cudaEventRecord(d.pjoin, d.pst[1])) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(st, d.pjoin, 0)) != cudaSuccess) return e;
+  if ((e = cudaStreamWaitEvent(st, d.pev_z[nch - 1], 0)) != cudaSuccess) return e;
+  return launch_xinv<C>(g, d, L, A, out, inv_planes * g.tc[1], 0, axpby, alpha, beta, st, ls);
+}
+
 template <typename C>
 cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, const C* in, C* out, C* A, C* B,
                           int nrhs, bool axpby, C alpha, C beta, cudaStream_t st, const LsEpi<C>* ls) {
+  const int nch = kx_chunks<C>(g, d, L, nrhs);
+  if (nch > 1) return launch_matvec_pipe<C>(g, d, L, in, out, A, B, nrhs, axpby, alpha, beta, st, ls, nch);
   for (int ph = 0; ph < 3; ++ph) {
     cudaError_t e = launch_matvec_phase<C>(ph, g, d, L, in, out, A, B, nrhs, axpby, alpha, beta, st, ls);
     if (e != cudaSuccess) return e;
@@ -3054,8 +3163,10 @@ cudaError_t launch_matvec(const Geom& g, const DevOp<C>& d, const Launch& L, con
   template cudaError_t launch_xfwd<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
                                       cudaStream_t);                                                              \
   template cudaError_t launch_y<C>(const Geom&, const DevOp<C>&, const Launch&, bool, const C*, C*, int64_t,      \
-                                   int64_t, int64_t, int64_t, cudaStream_t);                                      \
-  template cudaError_t launch_z<C>(const Geom&, const DevOp<C>&, const Launch&, C*, int, cudaStream_t);           \
+                                   int64_t, int64_t, int64_t, cudaStream_t, const KxChunk*);                      \
+  template cudaError_t launch_z<C>(const Geom&, const DevOp<C>&, const Launch&, C*, int, cudaStream_t,            \
+                                   const KxChunk*);                                                               \
+  template int kx_chunks<C>(const Geom&, const DevOp<C>&, const Launch&, int);                                    \
   template cudaError_t launch_xinv<C>(const Geom&, const DevOp<C>&, const Launch&, const C*, C*, int64_t,         \
                                       int64_t, bool, C, C, cudaStream_t, const LsEpi<C>*);
 
