@@ -41,7 +41,7 @@ CEL = (256, 256, 128)
 SWEEP_CEL = (128, 128, 64)
 SCL = ("1/32", "1/32", "1/32")
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-E2E_BATCH = 4  # host vectors (403 MB each) per API call in the end-to-end leg
+E2E_BATCH = 8  # host vectors (403 MB each) per API call in the end-to-end leg
 
 
 def bench_config(c64: bool, world: int) -> dict:

@@ -708,7 +708,7 @@ class SolveInfo:
 
 
 def solve(ls: LippmannSchwinger, i, *, tol: float = 1e-6, mixed: bool = False, ell: int = 2,
-          delta: float = 0.01, max_matvecs: int = 4000, max_restarts: int = 20, x0=None,
+          delta: float = 0.1, max_matvecs: int = 4000, max_restarts: int = 20, x0=None,
           graph: bool = True, check: bool = True, stream=None, keep: bool = False):
     """Solve ls * t = i (t = (1 - chi G)^-1 i, examples/scattering_film.jl:58-61)
     with BiCGStab(ell) on the GPU, for one field or a stack of nrhs fields.
@@ -802,7 +802,7 @@ class SolveServer:
         except Exception:
             pass
 
-    def submit(self, cel, scl, chi, b, *, tol: float = 1e-6, max_matvecs: int = 4000, delta: float = 0.01,
+    def submit(self, cel, scl, chi, b, *, tol: float = 1e-6, max_matvecs: int = 4000, delta: float = 0.1,
                max_restarts: int = 20) -> int:
         v = GlaVol(cel, scl).to_c()
         chi_a = np.asfortranarray(np.asarray(chi, dtype=np.complex128))

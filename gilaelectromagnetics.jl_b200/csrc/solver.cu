@@ -878,6 +878,7 @@ class LsBatchT final : public LsBatch {
     bool in_upd = false;      // part of the reliable update in flight
     double bn = 0, rn = 0, scale = 0, maxr = 0;
     int restarts = 0, cycles = 0, updates = 0, mv = 0;
+    int since_upd = 0;  // cycles since the last reliable update or (re)start
     SlotOpts o;
     void* x_out = nullptr;
     uint64_t tag = 0;
@@ -1141,12 +1142,17 @@ class LsBatchT final : public LsBatch {
       q.in_upd = false;
       if (!(q.state == 1 && q.iter)) continue;
       ++q.cycles;
+      ++q.since_upd;
       q.mv += mvc;
       q.pending = true;
       const Stat& s = st_h_[r];
       const double nr = std::sqrt(s.nrm2);
       const bool budget = q.mv + mvc > q.o.max_mv;
-      if (s.broke || !s.act || budget || (mixed && nr < q.o.delta * q.maxr)) {
+      // a residual drop of delta triggers an update only kReliableGap cycles
+      // after the last one: a system that converges by 10x per cycle would
+      // otherwise pay one FP64 matvec per cycle of 2l ComplexF32 ones
+      const bool drop = mixed && nr < q.o.delta * q.maxr && q.since_upd >= kReliableGap;
+      if (s.broke || !s.act || budget || drop) {
         m[r] = 1;
         mh[r] = 1;
         q.in_upd = true;
@@ -1176,6 +1182,7 @@ class LsBatchT final : public LsBatch {
       if (!q.in_upd) continue;
       q.in_upd = false;
       q.pending = false;
+      q.since_upd = 0;
       ++q.updates;
       q.rn = std::sqrt(ph(3)[r]);
       Stat& s = st_h_[r];
@@ -1410,7 +1417,7 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   so.tol = opts && opts->tol > 0 ? opts->tol : 1e-6;
   so.max_mv = opts && opts->max_matvecs > 0 ? opts->max_matvecs : 4000;
   so.max_restarts = opts && opts->max_restarts > 0 ? opts->max_restarts : 20;
-  so.delta = opts && opts->delta > 0 ? opts->delta : 0.01;
+  so.delta = opts && opts->delta > 0 ? opts->delta : 0.1;
   so.x0 = opts ? (opts->x0 != 0) : 0;
   if (cfg.ell > 4) return fail(GILA_ERR_ARG, "BiCGStab(l) degree must be 1..4");
   Core* inner = nullptr;

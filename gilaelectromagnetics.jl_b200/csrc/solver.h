@@ -11,9 +11,12 @@
 namespace gila {
 
 // per right-hand side stopping rules
+// cycles between two reliable updates triggered by the residual drop delta
+constexpr int kReliableGap = 3;
+
 struct SlotOpts {
   double tol = 1e-6;     // FP64 relative residual target
-  double delta = 0.01;   // mixed: recursive-residual drop that triggers a reliable update
+  double delta = 0.1;    // mixed: recursive-residual drop that triggers a reliable update
   int max_mv = 4000;     // Krylov operator applications
   int max_restarts = 20; // Krylov (re)starts
   int x0 = 0;            // x_out holds an initial guess

@@ -140,6 +140,9 @@ def bicgstabl(apply, b: np.ndarray, ell: int = 2, reltol: float = np.sqrt(np.fin
     return k.x, {"iters": it, "mv": mv, "nrm": nrm, "broke": state == "broke"}
 
 
+RELIABLE_GAP = 3  # cycles between two updates triggered by the residual drop delta
+
+
 def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inner_apply=None,
                    delta: float = 0.1, max_mv: int = 4000, max_restarts: int = 20, rs=None):
     """The GPU solver's algorithm: BiCGStab(l) on `inner_apply` (FP64
@@ -148,8 +151,9 @@ def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inne
 
     The Krylov process runs on the scaled system A d = r / s (s = |r| at its
     start).  After a cycle whose recursive residual fell below delta times
-    its largest value since the last update (mixed only; delta = 0 for the
-    plain solve), claimed convergence (0.9 tol |b| / s), or broke down: the
+    its largest value since the last update, at least RELIABLE_GAP cycles
+    after that update (mixed only; delta = 0 for the plain solve), claimed
+    convergence (0.9 tol |b| / s), or broke down: the
     correction is folded into the FP64 solution, x += s d, d = 0, and the
     recursive residual is replaced by the FP64 one, r = (b - A64 x) / s,
     keeping the search directions.  A breakdown, or claimed convergence that
@@ -178,13 +182,15 @@ def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inne
             s = rn
             k = _Krylov(inner, r / s, ell, rs)
             maxr = 1.0
+            since = 0
             info["restarts"] += 1
         if mv + 2 * ell > max_mv:
             break
         nrm, state = k.cycle(0.9 * tol * bn / s)
         mv += 2 * ell
         info["iters"] += 1
-        if state == "ok" and not nrm < d * maxr:
+        since += 1
+        if state == "ok" and not (nrm < d * maxr and since >= RELIABLE_GAP):
             maxr = max(maxr, nrm)
             continue
         x = x + s * k.x                      # reliable update
@@ -192,6 +198,7 @@ def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inne
         r = b - apply64(x)
         rn = np.linalg.norm(r)
         info["updates"] += 1
+        since = 0
         if state == "ok":
             k.R[0] = r / s
             maxr = rn / s
