@@ -757,7 +757,8 @@ def cpu_baseline():
     dt = time.perf_counter() - t0
     return {"value": round(1 / dt, 4), "unit": "matvec/s", "cores": n, "kind": "port",
             "sample": f"1 matvec of the same 256x256x128 ComplexF64 self operator (numpy/scipy.fft "
-                      f"restatement of egoBrnHst!, FFT workers={n}, elementwise steps single-threaded)"}, x, y
+                      f"restatement of egoBrnHst!: FFT workers={n}, the recursion's branches on concurrent threads "
+                      f"as the reference spawns them)"}, x, y
 
 
 def oracle_check(gila, x, y_ref):
@@ -833,7 +834,8 @@ def run_reference(a, world):
     dt = time.perf_counter() - t0
     val = k / dt
     sample = (f"{k} of {a.steps} requested steps timed after 1 warm-up (1 matvec each; the rest skipped to bound "
-              f"the CPU run), numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n}")
+              f"the CPU run), numpy/scipy.fft restatement of egoBrnHst! with FFT workers={n} and the recursion's "
+              f"branches on concurrent threads")
     out = {"impl": "reference", "metric": METRIC if a.dtype == "c128" else METRIC.replace("ComplexF64", "ComplexF32"),
            "value": round(val, 4), "unit": "matvec/s", "n_gpus": world,
            "steps": a.steps, "warmup": a.warmup, "ms_per_step": round(dt / k * 1e3, 2), "higher_is_better": True,

@@ -31,16 +31,22 @@ from .gla_mem import ExtInf
 
 _fft = np.fft.fft
 _ifft = np.fft.ifft
+_parallel = False
 
 
 def use_fft_workers(n: int) -> None:
-    """Run the 1-D transforms with scipy.fft on n threads (the reference runs
-    FFTW with FFTW.set_num_threads(nthreads()), test/preamble.jl:1-14); the
-    elementwise split / merge / multiply steps stay single-threaded numpy."""
-    global _fft, _ifft
+    """Run the host path on n threads as the reference does: the 1-D
+    transforms with scipy.fft on n threads (the reference runs FFTW with
+    FFTW.set_num_threads(nthreads()), test/preamble.jl:1-14), and the two
+    branches of every level of the recursion concurrently, so that the eight
+    leaves run at once (egoBrnHst! spawns them, src/glaAct.jl:122-131); numpy
+    releases the interpreter lock inside its array operations, so the
+    branches' split / multiply / merge steps overlap."""
+    global _fft, _ifft, _parallel
     import scipy.fft as sfft
     _fft = lambda a, axis: sfft.fft(a, axis=axis, workers=n)  # noqa: E731
     _ifft = lambda a, axis: sfft.ifft(a, axis=axis, workers=n)  # noqa: E731
+    _parallel = n > 1
 
 
 class OprMem:
@@ -234,8 +240,15 @@ def _brn(mem: OprMem, lvl: int, bid: int, act: np.ndarray) -> np.ndarray:
             prg_e = np.empty(psz, dtype=mem.dtype)
             prg_o = np.empty(psz, dtype=mem.dtype)
             _spt_ext(prg_e, prg_o, ax, mem.phz[ax], mix, org)
-        eve = _brn(mem, lvl + 1, bid, prg_e)
-        odd = _brn(mem, lvl + 1, _nxt(lvl, bid), prg_o)
+        if _parallel:
+            from concurrent.futures import ThreadPoolExecutor
+            with ThreadPoolExecutor(2) as ex:
+                fe = ex.submit(_brn, mem, lvl + 1, bid, prg_e)
+                fo = ex.submit(_brn, mem, lvl + 1, _nxt(lvl, bid), prg_o)
+                eve, odd = fe.result(), fo.result()
+        else:
+            eve = _brn(mem, lvl + 1, bid, prg_e)
+            odd = _brn(mem, lvl + 1, _nxt(lvl, bid), prg_o)
         if eve.shape[ax] == mix.trg_cel[ax]:
             shp = [1] * 5
             shp[ax] = -1
