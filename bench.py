@@ -338,8 +338,9 @@ def main():
     achieved = zb / (passes[1] / 1e3) / 1e9
     traffic = ncu_traffic(f"z_pass_{a.dtype}_256x256x128")
     roofline = {"bound": "hbm",
-                "kernel": ("k_zf2_ct" if f32 else "k_zf_ct") + " (z pencils: forward FFT, 3x3 multiply fused with "
-                          "the last / first butterflies, inverse FFT)",
+                "kernel": f"{'k_zg2_ct' if f32 else 'k_zg_ct'}<{2 * CEL[2]},{mem.tiles[3]}>" + " (z pencils: register-fed forward "
+                          "FFT, 3x3 multiply fused with the last / first butterflies, inverse FFT truncated to the "
+                          "target)",
                 "achieved": round(achieved, 1), "peak": peak, "peak_kind": peak_kind, "unit": "GB/s",
                 "frac": round(achieved / peak, 4), "traffic": traffic,
                 "algorithmic_bytes_per_launch": zb, "launch_ms": round(passes[1], 4),
