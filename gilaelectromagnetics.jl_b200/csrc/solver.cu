@@ -1448,6 +1448,13 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   cudaStream_t st = bt->stream();
   cudaStream_t user = static_cast<cudaStream_t>(stream);
   cudaEvent_t ev = nullptr;
+  // the ordering event is destroyed on every exit
+  struct EvGuard {
+    cudaEvent_t* e;
+    ~EvGuard() {
+      if (*e) cudaEventDestroy(*e);
+    }
+  } ev_guard{&ev};
   if (user) {
     GILA_CUDA_TRY(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
     GILA_CUDA_TRY(cudaEventRecord(ev, user));
@@ -1485,7 +1492,6 @@ gila_status gila_ls_solve(gila_opr* g64, gila_opr* g32, const void* chi, const v
   if (ev) {
     cudaEventRecord(ev, st);
     cudaStreamWaitEvent(user, ev, 0);
-    cudaEventDestroy(ev);
   }
   if (keep) {
     std::lock_guard<std::mutex> lk(a.mu);

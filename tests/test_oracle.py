@@ -128,3 +128,22 @@ def test_kernel_build_oracle_relations():
     yE = ego_opr(OprMem(mixE, furE), xA)
     assert rel_l2(yE, yU[:, 4:]) < 1e-12
     assert np.abs(crcU[0, 1] - crcU[1, 0]).max() < 1e-12 * np.abs(crcU[0, 1]).max()
+
+
+def test_threaded_host_path_matches_sequential():
+    """The timed CPU baseline runs the restatement with scipy.fft workers and
+    the recursion's branches on threads (as egoBrnHst! spawns them); the
+    values must be those of the sequential restatement."""
+    import oracle.matvec as om
+    from oracle.synth import seeded_current, synth_operator
+    mix, fur, _, _, _, _ = synth_operator((10, 8, 6), ("1/32", "1/32", "1/32"))
+    mem = om.OprMem(mix, fur)
+    x = seeded_current(mix.src_cel, 3)
+    seq = om.ego_opr(mem, x)
+    saved = (om._fft, om._ifft, om._parallel)
+    try:
+        om.use_fft_workers(4)
+        par = om.ego_opr(mem, x)
+    finally:
+        om._fft, om._ifft, om._parallel = saved
+    assert np.allclose(par, seq, rtol=0, atol=1e-13 * np.abs(seq).max())
