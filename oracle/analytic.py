@@ -1,5 +1,6 @@
 """Analytic checks of the Green operator's physics: the point-dipole field,
-passivity and reciprocity of the dense operator.
+passivity and reciprocity of the dense operator, and the Galerkin cell-pair
+blocks by direct quadrature.
 
 TEST INFRASTRUCTURE ONLY (see oracle/__init__.py).
 
@@ -15,7 +16,8 @@ leaves commented out (test/runtests.jl:103-113):
                              agreeing to 1e-8 (kerbuild.weak / the GPU
                              entry point do the evaluation).
 The functions here restate the arithmetic of the first two so that the tests
-can assert on it.
+can assert on it.  The dipole check leaves out the cells within two of the
+dipole; the cell-pair blocks (below) check those near-field entries too.
 """
 from __future__ import annotations
 
@@ -110,3 +112,74 @@ def anti_hermitian_eigs(M: np.ndarray, frq: complex = 1.0 + 0j) -> np.ndarray:
     (i/2) conj(f^2) M^H - (i/2) f^2 M, a Hermitian matrix."""
     asm = 0.5j * np.conj(frq ** 2) * M.conj().T - 0.5j * frq ** 2 * M
     return np.linalg.eigvalsh(0.5 * (asm + asm.conj().T))
+
+
+# --------------------------------------------------------- cell-pair blocks
+# The operator's 3x3 block between a source cell and a target cell is the
+# Galerkin integral (1/V) int_target int_source G(r - r') dr' dr of the
+# dipole field G above (a unit current in the source cell; the dipole test
+# feeds 1/V).  Its imaginary part is an entire function of r - r',
+#     Im G(r) = 2 pi^2 [ (2 j0(s) - j2(s)) / 3 I + j2(s) r^ r^ ],  s = 2 pi |r|,
+# so a tensor Gauss-Legendre rule over both cubes converges to rounding for
+# every pair, touching and self pairs included; the real part,
+#     Re G(r) = 2 pi^2 [ (y2(s) - 2 y0(s)) / 3 I - y2(s) r^ r^ ],
+# is smooth only for cells that do not touch.  (j, y: spherical Bessel
+# functions; the two forms restate the bracket of egoAna! split into
+# e^{is}/s terms.)
+
+def green_part(d: np.ndarray, part: str) -> np.ndarray:
+    """Re or Im of G at separations d[..., 3] (wavelengths): [..., 3, 3]."""
+    from scipy.special import spherical_jn, spherical_yn
+    r = np.sqrt((d ** 2).sum(-1))
+    s = 2.0 * math.pi * r
+    out = np.zeros(d.shape[:-1] + (3, 3))
+    if part == "im":
+        j0 = spherical_jn(0, s)
+        small = s < 1e-3
+        ss = np.where(small, 1.0, s)
+        j2s2 = np.where(small, 1.0 / 15.0 - s ** 2 / 210.0, spherical_jn(2, ss) / ss ** 2)  # j2(s) / s^2
+        iso = (2.0 * j0 - j2s2 * s ** 2) / 3.0
+        for i in range(3):
+            for j in range(3):
+                out[..., i, j] = 2.0 * math.pi ** 2 * (iso * (i == j) + j2s2 * (2.0 * math.pi) ** 2 * d[..., i] * d[..., j])
+        return out
+    y0 = spherical_yn(0, s)
+    y2 = spherical_yn(2, s)
+    for i in range(3):
+        for j in range(3):
+            out[..., i, j] = 2.0 * math.pi ** 2 * ((y2 - 2.0 * y0) / 3.0 * (i == j) - y2 * d[..., i] * d[..., j] / r ** 2)
+    return out
+
+
+def cell_pair_block(off, h: float, part: str, n: int = 8) -> np.ndarray:
+    """(1/V) int int of Re or Im G over two cubes of side h whose centres are
+    off * h apart (target minus source), by an n-point Gauss-Legendre rule
+    per coordinate (n^6 point pairs)."""
+    x, w = np.polynomial.legendre.leggauss(n)
+    x = x * h / 2.0
+    w = w * h / 2.0
+    X, Y, Z = np.meshgrid(x, x, x, indexing="ij")
+    W = (w[:, None, None] * w[None, :, None] * w[None, None, :]).ravel()
+    P = np.stack([X.ravel(), Y.ravel(), Z.ravel()], -1)
+    d = (np.asarray(off, dtype=float) * h)[None, None, :] + P[:, None, :] - P[None, :, :]
+    return np.einsum("a,b,abij->ij", W, W, green_part(d, part)) / h ** 3
+
+
+# (target - source) cell offsets of the near-field check: self, face, edge
+# and vertex contact, and non-touching pairs
+NEAR_OFFSETS = [(0, 0, 0), (1, 0, 0), (0, 1, 1), (1, 1, 1), (2, 0, 0), (2, 1, 0), (0, 2, 2), (3, 1, 0), (2, -1, 1)]
+
+
+def operator_blocks(apply, cel, src_cell, offsets):
+    """3x3 blocks of the operator between src_cell and src_cell + off, from
+    three matvecs with unit currents (one per component)."""
+    cols = []
+    for j in range(3):
+        x = np.zeros((*cel, 3), dtype=np.complex128, order="F")
+        x[tuple(src_cell) + (j,)] = 1.0
+        cols.append(np.asarray(apply(x)))
+    out = {}
+    for off in offsets:
+        t = tuple(a + b for a, b in zip(src_cell, off))
+        out[off] = np.array([[cols[j][t + (i,)] for j in range(3)] for i in range(3)])
+    return out

@@ -7,6 +7,8 @@ oracle), plus the exact 32^3 workload end to end against the oracle:
   * test/anaTest.jl:10-106   dipole field vs the analytic Green function;
   * test/posDefTest.jl:10-29 passivity (and reciprocity) of the dense operator;
   * test/intConTest.jl:6-35  wekS / wekE / wekV converged at intOrd 32;
+  * the near-field blocks (self and contact pairs included) against direct
+    quadrature of the analytic Green function;
   * the 32^3 self operator of 1/32-wavelength cells: GPU build vs the C
     oracle's build, and its matvec on a seeded current vs the oracle's
     matvec, in ComplexF64 and ComplexF32.
@@ -21,7 +23,7 @@ from oracle import analytic as an
 from oracle import kerbuild as kb
 from oracle.matvec import OprMem, ego_opr
 from oracle.synth import seeded_current
-from test_physics_oracle import dipole_check
+from test_physics_oracle import assert_near_field, dipole_check, near_field_check
 
 pytestmark = pytest.mark.gpu
 
@@ -61,6 +63,23 @@ def test_gpu_passivity_and_reciprocity(cel, scl):
     assert ev.min() > -1e-6, ev.min()
     assert ev.max() > 1e-3
     assert np.linalg.norm(M - M.T) <= 1e-12 * np.linalg.norm(M)
+
+
+@pytest.mark.parametrize("dtype", [np.complex128, np.complex64], ids=["c128", "c64"])
+def test_gpu_near_field_blocks_match_quadrature(dtype):
+    """GPU build and GPU matvec.  In ComplexF32 the imaginary part (about
+    1/800 of the self block's real part) is held to FP32 rounding of the
+    largest entry, 2e-6 of it, and the far real part to the quadrature's
+    5e-5."""
+    gila = load_pkg()
+    mem = _build(gila, (8, 8, 8), ("1/32",) * 3, dtype)
+    rel, absl = near_field_check(lambda x: gila.egoOpr(mem, np.asfortranarray(x.astype(dtype))))
+    if dtype == np.complex128:
+        assert_near_field(rel)
+    else:
+        for off in rel:
+            assert absl[off][0] < 2e-6, (off, absl[off])
+            assert rel[off][1] is None or rel[off][1] < 5e-5, (off, rel[off])
 
 
 def test_gpu_weak_integrals_converge_and_match_oracle():

@@ -13,7 +13,13 @@ physics rather than to a second restatement of the same code:
   * passivity: the anti-Hermitian part of the dense operator has no
     eigenvalue below -1e-6, and the operator is reciprocal (M = M^T);
   * quadrature convergence: wekS / wekE / wekV at intOrd 32 and 40 agree to
-    1e-8.
+    1e-8;
+  * near field: the operator's 3x3 blocks between a cell and its neighbours
+    (self, face, edge and vertex contact, and non-touching pairs) against
+    the Galerkin double integral of the analytic Green function by direct
+    Gauss-Legendre quadrature -- the imaginary part, smooth everywhere, to
+    1e-10 for every pair; the real part, singular at contact, to 5e-5 for
+    the non-touching pairs (the weak-form cubature's tolerance is 1e-6).
 """
 from __future__ import annotations
 
@@ -76,3 +82,53 @@ def test_oracle_weak_integrals_converge():
     b = kb.weak(REF_SCL, int_ord=40)
     for x, y in zip(a, b):
         assert np.max(np.abs(x - y) / np.abs(y)) < 1e-8
+
+
+NEAR_CEL = (8, 8, 8)
+NEAR_SCL = ("1/32", "1/32", "1/32")
+NEAR_SRC = (2, 3, 3)
+
+
+def near_field_check(apply, cel=NEAR_CEL, scl=NEAR_SCL, src=NEAR_SRC):
+    """Per cell offset (Im error, Re error or None for touching pairs), each
+    relative to the largest entry of its quadrature block; and the same
+    errors relative to the largest entry of all the blocks (the real part of
+    the self block), the scale of a rounding error."""
+    from fractions import Fraction
+    h = float(Fraction(scl[0]))
+    blocks = an.operator_blocks(apply, cel, src, an.NEAR_OFFSETS)
+    scale = max(np.abs(b).max() for b in blocks.values())
+    rel, absl = {}, {}
+    for off, blk in blocks.items():
+        qi = an.cell_pair_block(off, h, "im")
+        di = np.abs(blk.imag - qi).max()
+        dr = er = None
+        if max(abs(o) for o in off) >= 2:
+            qr = an.cell_pair_block(off, h, "re")
+            dr = np.abs(blk.real - qr).max()
+            er = dr / np.abs(qr).max()
+        rel[off] = (di / np.abs(qi).max(), er)
+        absl[off] = (di / scale, None if dr is None else dr / scale)
+    return rel, absl
+
+
+def assert_near_field(errs):
+    for off, (ei, er) in errs.items():
+        assert ei < 1e-10, (off, ei)
+        assert er is None or er < 5e-5, (off, er)
+    assert sum(er is not None for _, er in errs.values()) >= 4
+
+
+def test_quadrature_blocks_converged():
+    h = 1.0 / 32
+    for off in [(0, 0, 0), (1, 1, 0)]:
+        a, b = an.cell_pair_block(off, h, "im", 6), an.cell_pair_block(off, h, "im", 8)
+        assert np.abs(a - b).max() < 1e-12 * np.abs(b).max()
+    a, b = an.cell_pair_block((2, 1, 0), h, "re", 8), an.cell_pair_block((2, 1, 0), h, "re", 10)
+    assert np.abs(a - b).max() < 1e-9 * np.abs(b).max()
+
+
+def test_oracle_near_field_blocks_match_quadrature():
+    mix, fur, _, _, _, _ = kb.build_operator(NEAR_CEL, NEAR_SCL, int_ord=32)
+    mem = OprMem(mix, fur)
+    assert_near_field(near_field_check(lambda x: ego_opr(mem, x))[0])
