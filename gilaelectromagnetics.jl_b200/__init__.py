@@ -21,6 +21,8 @@ The names, argument meanings and error behaviour follow the reference:
                                                    examples/GilaOperators.jl:57-96
   solve(ls, i)               BiCGStab(l) solve     examples/scattering_film.jl:58-61
   SolveServer                continuous-batching solve server (no reference counterpart)
+  SlabOpr                    one matvec split over the GPUs of a process group
+                             (slab decomposition; no reference counterpart)
 
 Vectors use the reference's memory layout: (Nx, Ny, Nz, 3) column-major.
 numpy arrays are passed as shape (Nx, Ny, Nz, 3) in Fortran order (or flat);
@@ -43,6 +45,7 @@ __all__ = [
     "isselfoperator", "isexternaloperator", "glaSze", "size", "eltype", "issymmetric",
     "isposdef", "ishermitian", "isdiag", "GilaError", "DimensionMismatch", "ArgumentError",
     "Context", "default_context", "cast", "weak_integrals", "LippmannSchwinger", "solve", "SolveInfo", "SolveServer",
+    "SlabOpr", "SlabPlan", "SlabPieces", "slab_ranges", "slab_apply_local",
 ]
 
 
@@ -834,3 +837,6 @@ class SolveServer:
         s = L.GilaServerStatsC()
         _check(L.lib().gila_server_stats_get(self._h, ct.byref(s)))
         return {k: getattr(s, k) for k, _ in s._fields_}
+
+
+from .slab import SlabOpr, SlabPieces, SlabPlan, slab_apply_local, slab_ranges  # noqa: E402

@@ -123,6 +123,10 @@ _SIGS = [
     ("gila_weak_integrals", ct.c_int, [ct.c_void_p, ct.c_int64 * 3, ct.c_int64 * 3, ct.c_double, ct.c_double,
                                        ct.c_int32, ct.c_double * 36]),
     ("gila_debug_fail_alloc", ct.c_int, [ct.c_int64]),
+    ("gila_opr_slab_dims", ct.c_int, [ct.c_void_p, ct.c_int64 * 5]),
+    ("gila_opr_slab_fwd", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p]),
+    ("gila_opr_slab_z", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_int64, ct.c_void_p]),
+    ("gila_opr_slab_inv", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p, ct.c_void_p]),
     ("gila_opr_apply_noalloc", ct.c_int, [ct.c_void_p, ct.c_int, ct.c_void_p, ct.c_int64, ct.c_void_p,
                                           ct.c_int64, ct.c_void_p]),
 ]

@@ -19,8 +19,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libgila_b200.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
-SOURCES = ["gila.cu", "matvec.cu", "matvec_c128.cu", "matvec_c64.cu", "noalloc.cu", "kerbuild.cu", "solver.cu",
-           "server.cu"]
+SOURCES = ["gila.cu", "matvec.cu", "matvec_c128.cu", "matvec_c64.cu", "noalloc.cu", "slab.cu", "kerbuild.cu",
+           "solver.cu", "server.cu"]
 HEADERS = ["fft.cuh", "fft_ct.cuh", "matvec.cuh", "matvec_impl.cuh", "internal.h", "solver.h"]
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

@@ -233,6 +233,7 @@ Core::~Core() {
   cudaFree(B);
   cudaFree(stage_in);
   cudaFree(stage_out);
+  cudaFree(slab_a);
   for (cudaStream_t x : {st_h2d, st_d2h})
     if (x) {
       cudaStreamSynchronize(x);

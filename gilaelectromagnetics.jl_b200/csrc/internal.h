@@ -100,6 +100,10 @@ struct Core {
   cudaStream_t pipe_st[2] = {nullptr, nullptr};
   cudaEvent_t pipe_ev_y[kMaxKxChunks] = {}, pipe_ev_z[kMaxKxChunks] = {};
   cudaEvent_t pipe_join = nullptr;
+  // x/y slab buffer of the slab pieces of a slab-decomposed matvec (sized
+  // for the caller's z slabs, not the whole volume; gila_opr_slab_*)
+  void* slab_a = nullptr;
+  int64_t slab_a_cap = 0;
   std::mutex mu;
   // a solve batch kept resident between gila_ls_solve calls (opts->keep)
   std::shared_ptr<LsBatch> ls_keep;

@@ -118,9 +118,11 @@ cudaError_t launch_xfwd(const Geom& g, const DevOp<C>& d, const Launch& L, const
 template <typename C>
 cudaError_t launch_y(const Geom& g, const DevOp<C>& d, const Launch& L, bool inv, const C* src, C* dst, int64_t q0,
                      int64_t nq, int64_t src_sub, int64_t dst_sub, cudaStream_t st, const KxChunk* ch = nullptr);
+// (ky0, nky >= 0: B holds only spectrum rows ky0 .. ky0 + nky - 1, each
+// plane nky rows of Px; the slab pieces of a slab-decomposed matvec)
 template <typename C>
 cudaError_t launch_z(const Geom& g, const DevOp<C>& d, const Launch& L, C* B, int nrhs, cudaStream_t st,
-                     const KxChunk* ch = nullptr);
+                     const KxChunk* ch = nullptr, int ky0 = 0, int nky = -1);
 // kx chunks the pipelined matvec uses for this operator and launch shape
 // (0: no pipeline)
 template <typename C>

@@ -328,6 +328,41 @@ gila_status gila_server_stats_get(gila_server* srv, gila_server_stats* out);
  * disarms.  Process-wide. */
 gila_status gila_debug_fail_alloc(int64_t n);
 
+/* Slab pieces of a matvec split over several GPUs (no counterpart in the
+ * reference, which runs a volume on one device: src/glaAct.jl:191-321).  One
+ * process per GPU holds the operator (the whole Fourier kernel); rank r
+ * keeps source z planes [zs_r, zs_r + nzs_r) of the input, target z planes
+ * [zt_r, zt_r + nzt_r) of the output and spectrum rows [ky_r, ky_r + nky_r)
+ * between the passes.  A matvec is slab_fwd on the rank's source planes, an
+ * all-to-all that gives every rank all source planes of its rows, slab_z on
+ * its rows, an all-to-all that gives every rank all rows of its target
+ * planes, and slab_inv on its target planes; the exchanges are the caller's
+ * (gila_b200.SlabOpr uses NCCL through torch.distributed).  The pieces run
+ * the per-line arithmetic of gila_opr_apply with the operator's launch
+ * choices (its defaults until it is applied or autotuned), so the result
+ * equals the single-GPU matvec bit for bit.  Operators with one source and
+ * one target partition; every pointer is device memory on the operator's
+ * GPU; pieces of one operator must be ordered (one stream): they share an
+ * x/y buffer.  stream == NULL runs on the operator's stream and waits.
+ *
+ * dims: Px, Py, Pz (padded transform lengths), nin (source z planes), nout
+ * (target z planes). */
+gila_status gila_opr_slab_dims(const gila_opr* opr, int64_t dims[5]);
+/* in: nz source planes, (srcCelX, srcCelY, nz, 3) column-major; bslab: 3 *
+ * nz planes of Py x Px (component-major, then z, then ky, kx fastest)
+ * receiving each plane's 2-D spectrum. */
+gila_status gila_opr_slab_fwd(gila_opr* opr, gila_dtype dtype, const void* in, int64_t nz, void* bslab,
+                              void* stream);
+/* bz: spectrum rows ky0 .. ky0 + nky - 1 of every z plane, planes of nky x
+ * Px; on entry component c's nin source planes start at c * nin planes, on
+ * return its nout target planes start at c * nout planes (3 * max(nin,
+ * nout) planes of room). */
+gila_status gila_opr_slab_z(gila_opr* opr, gila_dtype dtype, void* bz, int64_t ky0, int64_t nky, void* stream);
+/* bslab: 3 * nz target planes of Py x Px (component-major); out: nz target
+ * planes, (trgCelX, trgCelY, nz, 3) column-major. */
+gila_status gila_opr_slab_inv(gila_opr* opr, gila_dtype dtype, const void* bslab, int64_t nz, void* out,
+                              void* stream);
+
 /* A matvec that allocates no device memory.  This entry point has no
  * counterpart in the reference.  It computes out = G * in for one vector,
  * like gila_opr_apply, for callers that cannot let the library call
