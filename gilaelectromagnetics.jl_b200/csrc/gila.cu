@@ -399,7 +399,8 @@ bool is_device_ptr(const void* p) {
 }
 
 // Re-layout the reference egoFur (tx,ty,tz,6,parS,parT column-major, one
-// array per branch eo) into [parT][eo][tz][ty][6][tx] of the operator dtype.
+// array per branch eo) into target-partition blocks laid out by ker_index,
+// in the operator dtype.
 template <typename CT>
 static gila_status load_fur(Core& c, const void* const fur[8], gila_dtype fdt, std::vector<CT>& out) {
   const Geom& g = c.geom;
@@ -440,7 +441,7 @@ static gila_status load_fur(Core& c, const void* const fur[8], gila_dtype fdt, s
               }
               if (!std::isfinite(re) || !std::isfinite(im))
                 return fail(GILA_ERR_NAN, "Fourier information contains non-numeric values.");
-              const int64_t di = (((((int64_t)tp * 8 + eo) * tz + iz) * ty + iy) * 6 + cc) * tx + ix;
+              const int64_t di = (int64_t)tp * 8 * per + ker_index(eo, iz, iy, cc, ix, tx, ty, tz);
               out[di].x = (decltype(out[di].x))re;
               out[di].y = (decltype(out[di].y))im;
             }
@@ -1100,7 +1101,7 @@ gila_status gila_opr_export_fur(gila_opr* opr, void* const host_out[8]) {
           for (int iy = 0; iy < ty; ++iy)
             for (int ix = 0; ix < tx; ++ix) {
               const int64_t di = ((((int64_t)tp * c.parS) * 6 + cc) * tz + iz) * ty * (int64_t)tx + (int64_t)iy * tx + ix;
-              const int64_t si = (((((int64_t)tp * 8 + eo) * tz + iz) * ty + iy) * 6 + cc) * tx + ix;
+              const int64_t si = (int64_t)tp * 8 * tx * ty * tz * 6 + ker_index(eo, iz, iy, cc, ix, tx, ty, tz);
               memcpy(dst + di * cs, h.data() + si * cs, cs);
             }
   }

@@ -71,7 +71,7 @@ struct Core {
   Geom geom{};
   int parS = 1;
   AxisPlan plan[3]{};
-  void* ker = nullptr;  // device, [parT][8][tz][ty][6][tx] complex
+  void* ker = nullptr;  // device, complex, target-partition blocks laid out by ker_index (matvec.cuh)
   size_t ker_bytes = 0;
   int* maps[3] = {nullptr, nullptr, nullptr};
   AxisPlan* plan_d = nullptr;  // device copies of plan[3]

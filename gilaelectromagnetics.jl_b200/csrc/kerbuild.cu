@@ -1059,7 +1059,9 @@ __global__ void k_extract(const Z* __restrict__ crc, int Px, int Py, int Pz, int
   const int64_t vol = (int64_t)Px * Py * Pz;
   const int64_t n = (int64_t)8 * tz * ty * tx * 6;
   for (int64_t o = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; o < n; o += (int64_t)gridDim.x * blockDim.x) {
-    int64_t q = o;  // o = (((eo * tz + iz) * ty + iy) * 6 + c) * tx + ix
+    int64_t q = o;  // o = ker_index(eo, iz, iy, c, ix, ...) = ((((py,pz) tz + iz) ty + iy) 6 + c) tx + ix) 2 + px
+    const int px = (int)(q & 1);
+    q >>= 1;
     const int ix = (int)(q % tx);
     q /= tx;
     const int c = (int)(q % 6);
@@ -1067,8 +1069,8 @@ __global__ void k_extract(const Z* __restrict__ crc, int Px, int Py, int Pz, int
     const int iy = (int)(q % ty);
     q /= ty;
     const int iz = (int)(q % tz);
-    const int eo = (int)(q / tz);
-    const int px = (eo >> 2) & 1, py = (eo >> 1) & 1, pz = eo & 1;
+    const int e = (int)(q / tz);
+    const int py = (e >> 1) & 1, pz = e & 1;
     // the reference broadcasts a one-element branch slice over two entries
     const int hx = Px / 2 > 1 ? Px / 2 : 1, hy = Py / 2 > 1 ? Py / 2 : 1, hz = Pz / 2 > 1 ? Pz / 2 : 1;
     const int fx = 2 * (ix < hx ? ix : hx - 1) + px, fy = 2 * (iy < hy ? iy : hy - 1) + py,

@@ -65,11 +65,21 @@ struct KxChunk {
   int nts = -1;  // positions; < 0: all
 };
 
+// Index of stored kernel entry (branch eo = 4 px + 2 py + pz, iz, iy,
+// component c, ix) in one target partition's block: the layout is
+// [py,pz][tz][ty][6][tx][px] -- the two x parities of one stored x index side
+// by side, so that the consecutive kx of a z-pass tile, whose parity
+// alternates, read consecutive entries (whole 32-byte sectors) of one
+// component.  A block holds 8 * tz * ty * 6 * tx entries.
+__host__ __device__ inline int64_t ker_index(int eo, int iz, int iy, int c, int ix, int tx, int ty, int tz) {
+  return (((((int64_t)(eo & 3) * tz + iz) * ty + iy) * 6 + c) * tx + ix) * 2 + (eo >> 2);
+}
+
 // Per-axis plan (radix list), twiddle tables and kernel-address maps live on
 // the device; Dev bundles the pointers for one dtype.
 template <typename C>
 struct DevOp {
-  const C* ker;      // [parT][8][tz][ty][6][tx]
+  const C* ker;      // [parT] blocks laid out by ker_index
   const int* map[3]; // per axis, per frequency f: m | p<<29 | mirrored<<30
   const C* tw[3];    // P-point twiddle tables
   AxisPlan plan[3];          // host copies (launch decisions)

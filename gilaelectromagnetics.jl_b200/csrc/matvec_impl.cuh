@@ -201,8 +201,8 @@ __device__ __forceinline__ int tile_seq(int idx, int n) {
   return (idx % 2 == 0) ? k : n - 1 - k;
 }
 
-// Kernel values are read once per column and their L2 lines are shared by
-// the CTAs of the mirror columns, not by the threads of one CTA: the loads
+// FP64 kernel values are read once per column and their L2 lines are shared
+// by the CTAs of the mirror columns, not by the threads of one CTA: the loads
 // bypass L1 allocation (measured 3% faster z passes at 256x256x128 than
 // cached loads, whose fills share the L1 data path with the transposes).
 __device__ __forceinline__ double2 ld_nc_na(const double2* g) {
@@ -210,24 +210,25 @@ __device__ __forceinline__ double2 ld_nc_na(const double2* g) {
   asm("ld.global.nc.L1::no_allocate.v2.f64 {%0, %1}, [%2];" : "=d"(r.x), "=d"(r.y) : "l"(g));
   return r;
 }
-__device__ __forceinline__ float2 ld_nc_na(const float2* g) {
-  float2 r;
-  asm("ld.global.nc.L1::no_allocate.v2.f32 {%0, %1}, [%2];" : "=f"(r.x), "=f"(r.y) : "l"(g));
-  return r;
-}
+// FP32: cached (measured faster than loads past L1 here), since a line-pair
+// thread reads the two x parities of one stored index, which sit side by
+// side: one 16-byte load where both are unmirrored, two loads of one line
+// otherwise
+__device__ __forceinline__ float2 ld_nc_na(const float2* g) { return __ldg(g); }
 template <typename C>
 __device__ __forceinline__ C ker_ld(const C* __restrict__ g, int c, int tx) {
-  return ld_nc_na(g + c * tx);
+  return ld_nc_na(g + 2 * c * tx);
 }
-// Stored kernel layout [parT][eo][tz][ty][6][tx]: for one stored (z, y) row
-// the six components are consecutive runs over x, so the threads of a warp
-// (consecutive kx of a tile) read consecutive entries of one component.
-// Returns the address of component 0 of entry (eo, iz, iy, ix).
+// Stored kernel layout: target-partition blocks laid out by ker_index
+// ([py,pz][tz][ty][6][tx][px]); the threads of a warp (consecutive kx of a
+// tile, alternating x parity) read consecutive entries of one component.
+// Returns the address of component 0 of entry (eo, iz, iy, ix); component c
+// is 2 * c * tx entries further (ker_ld).
 template <typename C>
 __device__ __forceinline__ const C* ker_at(const C* __restrict__ kpar, int eo, int iz, int iy, int ix, int tx, int ty,
                                            int tz) {
   // one partition holds 8 * tz * ty * 6 * tx < 2^31 entries (host-checked)
-  return kpar + ((((eo * tz + iz) * ty + iy) * 6) * tx + ix);
+  return kpar + (((((eo & 3) * tz + iz) * ty + iy) * 6) * tx + ix) * 2 + (eo >> 2);
 }
 
 
@@ -2086,10 +2087,18 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), GILA_ZF2_CAP ? zf2_min_blo
         Bfly<RL, false, C>::run(b[c], tw, TPL);
       }
     }
-    // the two columns kx0 + 2 lp (even parity) and kx0 + 2 lp + 1 (odd)
+    // the two columns kx0 + 2 lp (even parity) and kx0 + 2 lp + 1 (odd; on
+    // an odd-length x axis the last pair's second column lies outside the
+    // spectrum and reads the first column's entry, never stored)
     int pxa, ixa, rxa, pxb, ixb, rxb;
     ax_map(p.ax[0], kx0 + 2 * lp, pxa, ixa, rxa);
-    ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+    if (2 * lp + 1 < tmax) {
+      ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+    } else {
+      pxb = pxa;
+      ixb = ixa;
+      rxb = rxa;
+    }
 #pragma unroll
     for (int r = 0; r < RL; ++r) {
       const int kz = j + r * TPL;
@@ -2312,21 +2321,43 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), zf2_min_blocks(ct_threads2
       // the two columns kx0 + 2 lp (even parity) and kx0 + 2 lp + 1 (odd)
       int pxa = 0, ixa = 0, rxa = 0, pxb = 0, ixb = 0, rxb = 0;
       ax_map(p.ax[0], kx0 + 2 * lp, pxa, ixa, rxa);
-      ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+      // an odd-length x axis leaves the last pair's second column outside
+      // the spectrum: it reads the first column's entry (never stored)
+      if (2 * lp + 1 < tmax) {
+        ax_map(p.ax[0], kx0 + 2 * lp + 1, pxb, ixb, rxb);
+      } else {
+        pxb = pxa;
+        ixb = ixa;
+        rxb = rxa;
+      }
       // the first frequency's kernel values (both columns) go out before the barrier
       C ga[6], gb[6];
       int rz = 0;
-      if (live) {
+      // both columns' kernel values for z frequency f: the even and odd x
+      // parity of one unmirrored stored index are adjacent (one 16-byte load
+      // per component), mirrored ones are not
+      const bool adj = ixa == ixb && pxa == 0 && pxb == 1;
+      auto kload2 = [&](int f, int& rzf) {
         int pz, iz;
-        ax_map(p.ax[2], j, pz, iz, rz);
+        ax_map(p.ax[2], f, pz, iz, rzf);
         const C* gpa = ker_at(p.ker, 4 * pxa + 2 * py + pz, iz, iy, ixa, tx, ty, tz);
-        const C* gpb = ker_at(p.ker, 4 * pxb + 2 * py + pz, iz, iy, ixb, tx, ty, tz);
+        if (adj) {
 #pragma unroll
-        for (int q = 0; q < 6; ++q) {
-          ga[q] = ker_ld(gpa, q, tx);
-          gb[q] = ker_ld(gpb, q, tx);
+          for (int q = 0; q < 6; ++q) {
+            const float4 v = __ldg(reinterpret_cast<const float4*>(gpa + 2 * q * tx));
+            ga[q] = make_float2(v.x, v.y);
+            gb[q] = make_float2(v.z, v.w);
+          }
+        } else {
+          const C* gpb = ker_at(p.ker, 4 * pxb + 2 * py + pz, iz, iy, ixb, tx, ty, tz);
+#pragma unroll
+          for (int q = 0; q < 6; ++q) {
+            ga[q] = ker_ld(gpa, q, tx);
+            gb[q] = ker_ld(gpb, q, tx);
+          }
         }
-      }
+      };
+      if (live) kload2(j, rz);
       if (k == 0) __syncthreads();
       if (!live) continue;
       C a[3][RL], b[3][RL];
@@ -2354,17 +2385,7 @@ __global__ void __launch_bounds__(ct_threads2(TX, P), zf2_min_blocks(ct_threads2
       }
 #pragma unroll
       for (int r = 0; r < RL; ++r) {
-        if (r > 0) {
-          int pz, iz;
-          ax_map(p.ax[2], j + r * TPL, pz, iz, rz);
-          const C* gpa = ker_at(p.ker, 4 * pxa + 2 * py + pz, iz, iy, ixa, tx, ty, tz);
-          const C* gpb = ker_at(p.ker, 4 * pxb + 2 * py + pz, iz, iy, ixb, tx, ty, tz);
-#pragma unroll
-          for (int q = 0; q < 6; ++q) {
-            ga[q] = ker_ld(gpa, q, tx);
-            gb[q] = ker_ld(gpb, q, tx);
-          }
-        }
+        if (r > 0) kload2(j + r * TPL, rz);
         zmul3f(a[0][r], a[1][r], a[2][r], ga, rxa, ry, rz, s);
         zmul3f(b[0][r], b[1][r], b[2][r], gb, rxb, ry, rz, s);
       }
