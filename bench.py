@@ -41,7 +41,7 @@ CEL = (256, 256, 128)
 SWEEP_CEL = (128, 128, 64)
 SCL = ("1/32", "1/32", "1/32")
 L2_FLUSH_BYTES = 256 << 20  # > 126 MB L2
-E2E_BATCH = 16  # host vectors (403 MB each) per API call in the end-to-end leg
+E2E_BATCH = 32  # at most this many host vectors (403 MB each) per API call in the end-to-end leg
 
 
 def bench_config(c64: bool, world: int) -> dict:
@@ -308,8 +308,9 @@ def main():
     # uploads each vector, applies G and downloads the result, overlapping
     # the copies of neighbouring vectors with the passes, and returns when
     # the results are in host memory.
-    # 16 host vectors per call on one GPU (12.9 GB pinned); 4 per rank when
-    # several ranks share the host
+    # all timed vectors in one call on one GPU (up to 32: 25.8 GB pinned), so
+    # that only one upload and one download per call go unoverlapped; 4 per
+    # rank when several ranks share the host
     kb = max(1, min(E2E_BATCH if world == 1 else 4, a.steps))
     xh = torch.randn((kb, 3, CEL[2], CEL[1], CEL[0]), dtype=tdt).pin_memory()
     yh = torch.empty_like(xh).pin_memory()
