@@ -240,7 +240,7 @@ typedef struct {
                            the FP64 residual does not confirm); 0 -> 20 */
   double delta;         /* mixed: a reliable update follows a cycle whose recursive residual fell
                            below delta times its largest value since the last update, at least
-                           3 cycles after that update; <= 0 -> 0.1 */
+                           8 cycles after that update; <= 0 -> 0.1 */
   int32_t x0;           /* 1: x holds an initial guess on entry; 0: start from zero (as
                            IterativeSolvers.bicgstabl(A, b) does) */
   int32_t no_graph;     /* 1: launch every Krylov cycle's kernels directly instead of replaying

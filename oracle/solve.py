@@ -140,7 +140,7 @@ def bicgstabl(apply, b: np.ndarray, ell: int = 2, reltol: float = np.sqrt(np.fin
     return k.x, {"iters": it, "mv": mv, "nrm": nrm, "broke": state == "broke"}
 
 
-RELIABLE_GAP = 3  # cycles between two updates triggered by the residual drop delta
+RELIABLE_GAP = 8  # cycles between two updates triggered by the residual drop delta (solver.h kReliableGap)
 
 
 def reliable_solve(apply64, b: np.ndarray, tol: float = 1e-6, ell: int = 2, inner_apply=None,

@@ -87,7 +87,10 @@ def test_mixed_solve_reaches_fp64_residual(sys_):
     gila, G, ls, mem, chi, A = sys_
     b = _plane_wave(CEL)
     x, info = gila.solve(ls, b, tol=TOL, mixed=True)
-    assert info.converged == 1 and info.matvecs_f32 > 0 and info.outer >= 2
+    # convergence is declared only after an FP64 residual (a reliable update)
+    # confirms it; residual-drop updates come at most every kReliableGap
+    # cycles, so a short solve may need no other
+    assert info.converged == 1 and info.matvecs_f32 > 0 and info.outer >= 1 and info.matvecs_f64 >= 1
     # reliable updates keep the Krylov space: the ComplexF32 process needs
     # about as many iterations as the FP64 one
     _, ip = gila.solve(ls, b, tol=TOL)
