@@ -145,8 +145,8 @@ __device__ __forceinline__ double2 rounded(double2 v) {
 // part[r][0][blk] = sum_i conj(shadow[i]) b_r[i] over W-value units
 template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_sdot(const C* __restrict__ a, const C* __restrict__ b, int64_t n,
-                                             double2* __restrict__ part) {
-  const int r = blockIdx.y, nb = gridDim.x;
+                                             double2* __restrict__ part, const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.y] : blockIdx.y, nb = gridDim.x;
   b += n * r;
   double2 acc[1] = {make_double2(0.0, 0.0)};
   const int64_t nu = n / W;
@@ -162,8 +162,9 @@ __global__ void __launch_bounds__(kT) k_sdot(const C* __restrict__ a, const C* _
 
 // Gram matrix r_a^H r_b, a <= b <= ell, of the MR step (all kGram slots).
 template <typename C, int W>
-__global__ void __launch_bounds__(kT) k_gram(KVec<C> v, int ell, int64_t n, double2* __restrict__ part) {
-  const int r = blockIdx.y, nb = gridDim.x;
+__global__ void __launch_bounds__(kT) k_gram(KVec<C> v, int ell, int64_t n, double2* __restrict__ part,
+                                             const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.y] : blockIdx.y, nb = gridDim.x;
   const int64_t off = (int64_t)r * n / W;
   double2 acc[kGram];
 #pragma unroll
@@ -200,8 +201,9 @@ enum FinMode : int { FIN_STORE = 0, FIN_CHECK = 1, FIN_RESID = 2, FIN_NORM = 3 }
 // broken right-hand sides; FIN_NORM stores the squared norm in nrm_out.
 __global__ void __launch_bounds__(kT) k_fin(const double2* __restrict__ part, int K, int nb, double2* sc, int slot,
                                             Stat* st, const double* __restrict__ tol2, int mode,
-                                            double* __restrict__ nrm_out = nullptr) {
-  const int r = blockIdx.x;
+                                            double* __restrict__ nrm_out = nullptr,
+                                            const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.x] : blockIdx.x;
   if (mode == FIN_RESID && !st[r].act) return;
   __shared__ double2 sh[kT / 32];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
@@ -321,8 +323,8 @@ __global__ void k_mr_solve(double2* sc, Stat* st, int ell, int nrhs) {
 // BiCG part, step j (1-based): u_q = r_q - beta u_q, q < j, beta = rho / sigma
 template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_bicg_u(KVec<C> v, int j, int64_t n, const double2* __restrict__ sc,
-                                               const Stat* __restrict__ st) {
-  const int r = blockIdx.y;
+                                               const Stat* __restrict__ st, const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.y] : blockIdx.y;
   if (!st[r].act) return;
   const double2 beta = cdiv(sc[(int64_t)r * kSlots + S_RHO], sc[(int64_t)r * kSlots + S_SIG]);
   const int64_t off = (int64_t)r * n / W, nu = n / W;
@@ -346,8 +348,9 @@ __global__ void __launch_bounds__(kT) k_bicg_u(KVec<C> v, int j, int64_t n, cons
 // rho - beta * rho_prev; with chi = 0 the first step converges exactly).
 template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_bicg_r(KVec<C> v, int j, int64_t n, const double2* __restrict__ sc,
-                                               const Stat* __restrict__ st, double2* __restrict__ part) {
-  const int r = blockIdx.y, nb = gridDim.x;
+                                               const Stat* __restrict__ st, double2* __restrict__ part,
+                                               const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.y] : blockIdx.y, nb = gridDim.x;
   if (!st[r].act) return;
   const double2 alpha = cdiv(sc[(int64_t)r * kSlots + S_RHO], sc[(int64_t)r * kSlots + S_SIG]);
   const int64_t off = (int64_t)r * n / W, nu = n / W;
@@ -380,8 +383,9 @@ __global__ void __launch_bounds__(kT) k_bicg_r(KVec<C> v, int j, int64_t n, cons
 // r_0 -= sum_k gamma_k r_k (k = 1..l), and the partial of |r_0|^2.
 template <typename C, int W>
 __global__ void __launch_bounds__(kT) k_mr_update(KVec<C> v, int ell, int64_t n, const double2* __restrict__ sc,
-                                                  const Stat* __restrict__ st, double2* __restrict__ part) {
-  const int r = blockIdx.y, nb = gridDim.x;
+                                                  const Stat* __restrict__ st, double2* __restrict__ part,
+                                                  const int* __restrict__ act = nullptr) {
+  const int r = act ? act[blockIdx.y] : blockIdx.y, nb = gridDim.x;
   if (!st[r].act) return;
   double2 g[kMaxEll];
 #pragma unroll
@@ -683,6 +687,8 @@ class LsBatchT final : public LsBatch {
     GILA_CUDA_TRY(mem_.alloc((void**)&pb_d_, pb_bytes()));
     GILA_CUDA_TRY(mem_.alloc_host((void**)&st_h_, (size_t)S_ * sizeof(Stat)));
     GILA_CUDA_TRY(mem_.alloc_host((void**)&pb_h_, pb_bytes()));
+    GILA_CUDA_TRY(mem_.alloc((void**)&act_d_, (size_t)S_ * sizeof(int)));
+    GILA_CUDA_TRY(mem_.alloc_host((void**)&act_h_, (size_t)S_ * sizeof(int)));
     memset(st_h_, 0, (size_t)S_ * sizeof(Stat));
     memset(pb_h_, 0, pb_bytes());
     const int nvec = 2 * cfg_.ell + 3;
@@ -1050,7 +1056,14 @@ class LsBatchT final : public LsBatch {
   // vector kernels cover all slots and skip inactive ones), ending with the
   // copy of the per-slot status to the host.
   gila_status body(const std::vector<char>& m) {
-    const dim3 gv(nb_, S_);
+    // the vector kernels run one block row per iterating slot (act_d_ maps
+    // row -> slot, written by enqueue_cycle for this pattern of slots): a
+    // batch with few of its slots iterating launches no blocks for the rest
+    int na = 0;
+    for (char c : m) na += c != 0;
+    if (na == 0) return GILA_OK;
+    const dim3 gv(nb_, na);
+    const int* act = act_d_;
     const int sb = (S_ + 127) / 128;
     double* tol2 = pd(0);
     gila_status st;
@@ -1058,23 +1071,23 @@ class LsBatchT final : public LsBatch {
     auto lsa = [&](const CI* in, CI* out) -> gila_status { return apply_runs<CI>(opi_, in, out, m, chii_); };
     k_iter_start<<<sb, 128, 0, s_>>>(sc_, st_d_, S_);
     for (int j = 1; j <= ell; ++j) {
-      GILA_VW(k_sdot, gv, shadow_, kv_.r[j - 1], n_, part_);
-      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_RHO, st_d_, tol2, FIN_CHECK);
-      GILA_VW(k_bicg_u, gv, kv_, j, n_, sc_, st_d_);
+      GILA_VW(k_sdot, gv, shadow_, kv_.r[j - 1], n_, part_, act);
+      k_fin<<<na, kT, 0, s_>>>(part_, 1, nb_, sc_, S_RHO, st_d_, tol2, FIN_CHECK, nullptr, act);
+      GILA_VW(k_bicg_u, gv, kv_, j, n_, sc_, st_d_, act);
       GILA_CUDA_TRY(cudaGetLastError());
       if ((st = lsa(kv_.u[j - 1], kv_.u[j])) != GILA_OK) return st;
-      GILA_VW(k_sdot, gv, shadow_, kv_.u[j], n_, part_);
-      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, S_SIG, st_d_, tol2, FIN_CHECK);
-      GILA_VW(k_bicg_r, gv, kv_, j, n_, sc_, st_d_, part_);
-      k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
+      GILA_VW(k_sdot, gv, shadow_, kv_.u[j], n_, part_, act);
+      k_fin<<<na, kT, 0, s_>>>(part_, 1, nb_, sc_, S_SIG, st_d_, tol2, FIN_CHECK, nullptr, act);
+      GILA_VW(k_bicg_r, gv, kv_, j, n_, sc_, st_d_, part_, act);
+      k_fin<<<na, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID, nullptr, act);
       GILA_CUDA_TRY(cudaGetLastError());
       if ((st = lsa(kv_.r[j - 1], kv_.r[j])) != GILA_OK) return st;
     }
-    GILA_VW(k_gram, gv, kv_, ell, n_, part_);
-    k_fin<<<S_, kT, 0, s_>>>(part_, kGram, nb_, sc_, S_GRAM, st_d_, tol2, FIN_STORE);
+    GILA_VW(k_gram, gv, kv_, ell, n_, part_, act);
+    k_fin<<<na, kT, 0, s_>>>(part_, kGram, nb_, sc_, S_GRAM, st_d_, tol2, FIN_STORE, nullptr, act);
     k_mr_solve<<<sb, 128, 0, s_>>>(sc_, st_d_, ell, S_);
-    GILA_VW(k_mr_update, gv, kv_, ell, n_, sc_, st_d_, part_);
-    k_fin<<<S_, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID);
+    GILA_VW(k_mr_update, gv, kv_, ell, n_, sc_, st_d_, part_, act);
+    k_fin<<<na, kT, 0, s_>>>(part_, 1, nb_, sc_, 0, st_d_, tol2, FIN_RESID, nullptr, act);
     GILA_CUDA_TRY(cudaGetLastError());
     GILA_CUDA_TRY(cudaMemcpyAsync(st_h_, st_d_, (size_t)S_ * sizeof(Stat), cudaMemcpyDeviceToHost, s_));
     return GILA_OK;
@@ -1083,6 +1096,10 @@ class LsBatchT final : public LsBatch {
   gila_status enqueue_cycle() {
     std::vector<char> m(S_, 0);
     for (int r = 0; r < S_; ++r) m[r] = sl_[r].state == 1 && sl_[r].iter;
+    int na = 0;
+    for (int r = 0; r < S_; ++r)
+      if (m[r]) act_h_[na++] = r;
+    if (na > 0) GILA_CUDA_TRY(cudaMemcpyAsync(act_d_, act_h_, (size_t)na * sizeof(int), cudaMemcpyHostToDevice, s_));
     std::vector<int> key;
     for (auto [r0, r1] : runs_of(m, S_)) {
       key.push_back(r0);
@@ -1232,6 +1249,10 @@ class LsBatchT final : public LsBatch {
   double2 *part_ = nullptr, *sc_ = nullptr;
   Stat *st_d_ = nullptr, *st_h_ = nullptr;
   char *pb_d_ = nullptr, *pb_h_ = nullptr;
+  // iterating slots of the cycle in flight, in slot order (row -> slot map
+  // of the cycle's vector kernels); the host copy is rewritten only after the
+  // previous cycle has completed
+  int *act_d_ = nullptr, *act_h_ = nullptr;
   KVec<CI> kv_{};
   CI* shadow_ = nullptr;
   cudaGraphExec_t graph_ = nullptr;
