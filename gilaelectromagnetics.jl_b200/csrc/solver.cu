@@ -1053,8 +1053,9 @@ class LsBatchT final : public LsBatch {
   }
 
   // One BiCGStab(l) cycle for the slots in `m` (matvecs over their runs; the
-  // vector kernels cover all slots and skip inactive ones), ending with the
-  // copy of the per-slot status to the host.
+  // vector kernels over the iterating slots only, and skip slots retired
+  // during the cycle), ending with the copy of the per-slot status to the
+  // host.
   gila_status body(const std::vector<char>& m) {
     // the vector kernels run one block row per iterating slot (act_d_ maps
     // row -> slot, written by enqueue_cycle for this pattern of slots): a
